@@ -1,0 +1,409 @@
+#!/usr/bin/env python3
+"""Ply-step throughput of the B200 engine (positions per second).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                    [--workload slice|mix] [--path plain|batched]
+
+Workloads (synthetic, seeded; there is no public dataset for this path):
+  slice  KRRRvKRRR, king slice 96 (wK c1, bK e6), N = 1,229,490,380
+         positions: one slice-ply (W step + L step, tb8gen_b200.plyjob) with
+         L_prev/W_prev Bernoulli(0.01) from seed 1, illegal positions cleared.
+  mix    96 king slices from seed 2 over KRRRvKRRR, KQRvKRRR and KQRRvKRR
+         with p in {0.001, 0.01, 0.05}; neighbour marks go to per-material
+         shared bitmaps (see plyjob).
+
+A step is one slice-ply of every slice of the workload.  `value` is the
+positions of all slices (all ranks) per second of device time, inputs
+resident in HBM.  `e2e` is the same metric through the public C ABI with
+the inputs copied from pinned host memory and the W/L results copied back
+inside the timed region.  With --gpus N (torchrun) every rank runs its own
+replica of the workload (the ply step has no exchange between slices of a
+step): weak scaling, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ply positions/s (bit-exact)"
+UNIT = "positions/s"
+ALG_BYTES_PER_POS = 0.875  # W step 0.5 B + L step 0.375 B per position
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="slice", choices=["slice", "mix"])
+    ap.add_argument("--path", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="target CPU time of the bounded CPU sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_spec(name):
+    if name == "slice":
+        return [("KRRRvKRRR", 96, 0.01, 1)]
+    import numpy as np
+
+    rng = np.random.default_rng(2)
+    mats = ["KRRRvKRRR", "KQRvKRRR", "KQRRvKRR"]
+    ps = [0.001, 0.01, 0.05]
+    out = []
+    for j in range(96):
+        out.append((mats[j % 3], int(rng.integers(0, 462)), ps[(j // 3) % 3], 2))
+    return out
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/traffic.json, written from an ncu capture), if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)
+        return d.get(kernel)
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------- engine arm
+def run_engine(a, rank, world, local):
+    import torch
+
+    import tb8gen_b200 as tbg
+    from tb8gen_b200.plyjob import MaterialPool, SlicePly
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    tbg.init()
+    tbg.set_stream(stream)
+    spec = workload_spec(a.workload)
+    pools = {}
+    jobs = []
+    for mat, s, p, seed in spec:
+        pool = None
+        if a.workload == "mix":
+            if mat not in pools:
+                pools[mat] = MaterialPool(mat, seed)
+            pool = pools[mat]
+        jobs.append(SlicePly(mat, s, p, seed + 1000 * rank, pool))
+    torch.cuda.synchronize()
+    positions = sum(j.positions for j in jobs)
+
+    phase_names = SlicePly.PHASES
+    ev = {ph: [] for ph in phase_names}
+
+    def step(timed_phases=False):
+        if a.path == "batched":
+            raise SystemExit("batched path not available in this build")
+        # phase order: all W scatters, all epilogues, all L scatters, all verifies
+        for ph in phase_names:
+            if timed_phases:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            for j in jobs:
+                getattr(j, ph)()
+            if timed_phases:
+                e1.record(stream)
+                ev[ph].append((e0, e1))
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # device-time throughput, inputs resident in HBM
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = tbg.launches()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(a.steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    launches = tbg.launches() - n0
+    ms = t0.elapsed_time(t1) / a.steps
+    clk = clocks.stop()
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+
+    # per-phase device times (separate pass, same work)
+    for _ in range(max(3, a.steps // 2)):
+        step(timed_phases=True)
+    torch.cuda.synchronize()
+    phase_ms = {ph: statistics.median(e0.elapsed_time(e1) for e0, e1 in ev[ph])
+                for ph in phase_names}
+
+    counts = [j.counts() for j in jobs[:4]]
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not a.no_e2e:
+        e2e = run_e2e(a, jobs, stream, positions)
+
+    value = positions * world / (ms / 1e3)
+    peak, peak_kind = measured_peak()
+    # dominant kernel and its roofline
+    dom = max(phase_ms, key=phase_ms.get)
+    per_pos = {"w_scatter": 0.125, "w_epilogue": 0.5, "l_scatter": 0.125, "l_verify": 0.25}
+    alg = per_pos[dom] * positions
+    achieved = alg / (phase_ms[dom] / 1e3) / 1e9
+    traffic = committed_traffic(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "alg_bytes_per_launch": int(alg), "traffic": traffic,
+                "step_alg_GBps": round(ALG_BYTES_PER_POS * positions / (ms / 1e3) / 1e9, 1),
+                "step_frac": round(ALG_BYTES_PER_POS * positions / (ms / 1e3) / 1e9 / peak, 4)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = run_cpu_baseline(a, jobs)
+
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded Bernoulli bitmaps, seeded 7-piece stub)",
+        "config": {"workload": a.workload, "path": a.path, "slices": len(jobs),
+                   "positions_per_step": positions,
+                   "materials": sorted({j.material for j in jobs}),
+                   "l2": "inputs larger than L2 (>=16 MB bitmaps, many per step)"},
+        "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+        "counts_first_jobs": counts,
+        "roofline": roofline, "gpu_launches": launches, "clocks": clk,
+        "e2e": e2e, "cpu_baseline": cpu,
+    }
+    return line
+
+
+def run_e2e(a, jobs, stream, positions):
+    """Same steps through the C ABI with inputs in pinned host memory:
+    per step H2D of L_prev, W_prev and wins_in of every slice, the ply, and
+    D2H of W(s), L(s) and wins(s)."""
+    import torch
+
+    host_in, host_out = [], []
+    for j in jobs:
+        host_in.append([t.cpu().pin_memory() for t in (j.L_prev, j.W_prev, j.wins_in)])
+        host_out.append([torch.empty(j.B, dtype=torch.uint8).pin_memory() for _ in range(3)])
+    h2d = sum(j.B * 3 for j in jobs)
+    steps = max(2, min(a.steps, 5))
+
+    def one():
+        for j, hi in zip(jobs, host_in):
+            j.L_prev.copy_(hi[0], non_blocking=True)
+            j.W_prev.copy_(hi[1], non_blocking=True)
+            j.wins_in.copy_(hi[2], non_blocking=True)
+        for ph in jobs[0].PHASES:
+            for j in jobs:
+                getattr(j, ph)()
+        for j, ho in zip(jobs, host_out):
+            ho[0].copy_(j.T, non_blocking=True)
+            ho[1].copy_(j.X, non_blocking=True)
+            ho[2].copy_(j.wins, non_blocking=True)
+
+    one()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": round(positions / (ms / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms, 3),
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "steps": steps}
+
+
+def cpu_oracle(material, nthreads):
+    from oracle import oracle as orc
+
+    if orc.ref_available():
+        return orc.Ref(material, nthreads), "reference"
+    return orc.Port(material), "port"
+
+
+def run_cpu_baseline(a, jobs, budget=None):
+    """The reference's CPU ply (oracle/_ref, all host cores) on a bounded
+    sample of the first job: sources restricted to a leading fraction of
+    the slice, time extrapolated to the whole slice."""
+    from oracle.plyjob_cpu import CpuSlicePly
+
+    budget = budget or a.cpu_seconds
+    cores = os.cpu_count() or 1
+    job = jobs[0]
+    O, kind = cpu_oracle(job.material, cores)
+    threads = getattr(O, "nthreads", 1)
+    frac = 0.002
+    c = CpuSlicePly(O, job, frac)
+    t = c.step()
+    scal = c.times["w_scatter"] + c.times["l_scatter"] + c.times["l_verify"]
+    fixed = c.times["w_epilogue"]
+    want = max(0.0, budget - fixed)
+    frac2 = min(1.0, max(frac, frac * want / max(scal, 1e-6)))
+    if frac2 > frac * 1.5:
+        c = CpuSlicePly(O, job, frac2)
+        t = c.step()
+        frac = frac2
+        scal = c.times["w_scatter"] + c.times["l_scatter"] + c.times["l_verify"]
+        fixed = c.times["w_epilogue"]
+    t_full = scal / frac + fixed
+    return {"value": round(job.positions / t_full, 1), "unit": UNIT, "cores": threads,
+            "kind": kind, "seconds_measured": round(t, 3),
+            "sample": (f"{job.material} slice {job.s}: scatter sources restricted to the first "
+                       f"{frac:.4f} of the slice, epilogue and verify over the whole slice; "
+                       f"scatter+verify time scaled by 1/{frac:.4f}"),
+            "phase_s": {k: round(v, 4) for k, v in c.times.items()}}
+
+
+def run_reference(a, rank, world, local):
+    """Reference arm: the reference's own CPU workers on the host cores."""
+    import torch
+
+    if rank != 0:
+        return None
+    import tb8gen_b200 as tbg
+    from tb8gen_b200.plyjob import MaterialPool, SlicePly
+
+    # Inputs are generated by the engine's seeded generator on the GPU (the
+    # same bitmaps the engine arm uses), then copied to the host.
+    torch.cuda.set_device(local)
+    tbg.init()
+    mat, s, p, seed = workload_spec(a.workload)[0]
+    pool = MaterialPool(mat, seed) if a.workload == "mix" else None
+    job = SlicePly(mat, s, p, seed, pool)
+    torch.cuda.synchronize()
+    per_step = []
+    info = None
+    for _ in range(a.warmup + a.steps):
+        info = run_cpu_baseline(a, [job], budget=min(a.cpu_seconds, 20.0))
+        per_step.append(job.positions / info["value"])
+    ts = per_step[a.warmup:] or per_step
+    tm = statistics.median(ts)
+    v = job.positions / tm
+    return {
+        "metric": METRIC, "value": round(v, 1), "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(tm * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded Bernoulli bitmaps, seeded 7-piece stub)",
+        "config": {"workload": a.workload, "slices": 1, "material": mat, "slice": s},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": info["cores"],
+                         "kind": info["kind"], "sample": info["sample"]},
+        "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    a = parse()
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if a.impl == "reference":
+            line = run_reference(a, rank, world, local)
+        else:
+            line = run_engine(a, rank, world, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,203 @@
+/*
+ * tbgpu -- B200 (sm_100a) engine for the per-king-slice ply step of the
+ * tb8gen retrograde generator, behind a plain C ABI.
+ *
+ * The reference runs its ply step as `static` workers driven by
+ * run_threaded(worker, work, false) (threads.c:266-289), with parameters in
+ * file-scope globals (g_pos, ii, capt_ii, pc_to_set, work_slice, ...) and
+ * the slice buffers in kslice_buf[]/kslice_sub_buf[] addressed through
+ * kslice_slot[] (kslice.c:23-28).  Each entry point below replaces one such
+ * call; the host schedule (calc_W_n / calc_L_n, tb8gen.c:943-1084) stays.
+ *
+ * Conventions
+ *  - Every function returns TBG_OK (0) or a negative tbg_status.  The
+ *    reference exits on failure; its host shim does exit(EXIT_FAILURE) on a
+ *    negative status.
+ *  - Bitmaps use the reference's byte layout: one bit per position,
+ *    LSB-first within bytes (kslice.h:30-55), rounded up to 64 bytes
+ *    (kslice.c:191-196).  Device pointers must be 16-byte aligned.
+ *  - The caller owns all device memory (it binds it with tbg_slot_bind /
+ *    tbg_sub_bind); the library allocates only its own small status and
+ *    counter words (and, in tbg_ply_batch, a work queue).
+ *  - Work is stream-ordered on the stream set by tbg_set_stream (default:
+ *    the legacy default stream).  Calls that return a count synchronise
+ *    with a bounded wait.  One host thread per library instance, like the
+ *    reference's single calling thread.
+ *  - Positions are indexed with 32-bit arithmetic when the slice size is
+ *    below 2^32 and 64-bit arithmetic otherwise.
+ */
+#ifndef TBGPU_H
+#define TBGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum tbg_status {
+  TBG_OK = 0,
+  TBG_ERR_ARG = -1,      /* invalid argument or misaligned pointer */
+  TBG_ERR_STATE = -2,    /* tbg_init not called / no material selected */
+  TBG_ERR_UNBOUND = -3,  /* a slice the call reads or writes has no bound buffer */
+  TBG_ERR_CUDA = -4,     /* CUDA runtime error (see tbg_last_error) */
+  TBG_ERR_NOMEM = -5,    /* the library could not allocate its own device words */
+  TBG_ERR_DEVICE = -6,   /* a kernel met an access outside the bound buffers and skipped it */
+  TBG_ERR_TIMEOUT = -7,  /* a bounded wait gave up; the stream may still be running */
+  TBG_ERR_RANGE = -8     /* a size beyond a stated limit */
+};
+
+/* struct IdxInfo, tb8gen.h:4-13 (same field order and types). */
+typedef struct tbg_idx_info {
+  int numsets;
+  uint64_t size;
+  uint64_t factor[6];
+  uint32_t subfactor[6];
+  int first[6];
+  int mult[6];
+  int last[6];
+} tbg_idx_info;
+
+/* struct Position, movegen.h:18-26, pawnless build (same layout). */
+typedef struct tbg_position {
+  uint64_t occ;
+  uint8_t sq[8], pt[8];
+  int num, stm;
+  int8_t pcs[2][8];
+} tbg_position;
+
+/* ---- set-up ---------------------------------------------------------- */
+
+/* Replaces the table set-up of main() (init_movegen, init_tables,
+ * init_indices; tb8gen.c:1279-1282): selects device 0 (or the current
+ * device) and uploads nothing yet.  Idempotent. */
+int tbg_init(void);
+
+/* Registers a material from the reference's own set-up (ii, capt_ii[],
+ * g_pos, pc_to_set: tb8gen.c:1329-1378).  ii->subfactor[0] may carry the
+ * reference's +64 guard (tb8gen.c:227).  Returns a material handle >= 0
+ * and makes it current, or a negative status. */
+int tbg_material_init(const tbg_idx_info *ii, const tbg_idx_info *capt_ii,
+                      const tbg_position *pos, const int *pc_to_set);
+
+/* Same, parsing a material string such as "KRRRvKRRR" exactly as main()
+ * does (tb8gen.c:1284-1378).  Returns a handle >= 0 or a negative status. */
+int tbg_material_from_name(const char *name);
+
+/* Makes material `mat` current for the per-slice calls. */
+int tbg_material_select(int mat);
+
+/* Geometry of the current material: slice size in positions, slice bitmap
+ * bytes (kslice_cache_lines << 6), sub buffer bytes per slice
+ * (max of sub_size[], kslice.c:219) and the byte offset of set k in it
+ * (sub_offset[], kslice.c:214-218). */
+int tbg_geometry(uint64_t *size, uint64_t *bytes, uint64_t *sub_bytes,
+                 uint64_t sub_offset[6], uint64_t capt_size[6]);
+
+/* Stream for all following work (a cudaStream_t; NULL = default). */
+int tbg_set_stream(void *stream);
+
+/* Seed and modulus (3 or 5) of the 7-piece WDL stub used by tbg_calc_sub. */
+int tbg_set_stub(uint64_t seed, int modulus);
+
+/* ---- slot map (kslice_slot / kslice_buf / kslice_sub_buf) ------------ */
+
+/* Binds a device bitmap of `bytes` bytes to slice s of the current
+ * material; s == -1 is the scratch slot (kslice_buf[19]).  NULL unbinds. */
+int tbg_slot_bind(int s, void *dev_bitmap, size_t bytes);
+
+/* Binds a device sub buffer (the five sub bitmaps of kslice_sub_buf use
+ * this layout: sets at sub_offset[k]) to slice s; s == -1 is the scratch
+ * slot's sub base (kslice_sub_get_base(-1), kslice.h:63-68). */
+int tbg_sub_bind(int s, void *dev_sub, size_t bytes);
+
+int tbg_unbind_all(void);
+
+/* ---- the ply step ---------------------------------------------------- */
+
+/* predecessors(stm, s), tb8gen.c:519-527: every set bit of the scratch
+ * slot (opponent to move, slice s) is unmoved by side stm; marks are ORed
+ * into slice s and the slices its king moves reach (all must be bound). */
+int tbg_predecessors(int stm, int s);
+
+/* predecessors_sub(stm, s, legality), tb8gen.c:397-414: uncaptures from
+ * the sub buffer bound to s (sets of colour stm^1) into slice s and its
+ * king-move slices. */
+int tbg_predecessors_sub(int stm, int s, int legality);
+
+/* check_successors(stm, s), tb8gen.c:653-661: candidates in the scratch
+ * slot are kept iff legal and every move leads to a bit set in the
+ * opponent's "wins" bound to s (and its king-move slices) or, for a
+ * capture, in the sub buffer bound there. */
+int tbg_check_successors(int stm, int s);
+
+/* check_successors with the survivors written to dev_out (the bound
+ * bitmap size) instead of in place; the candidates are left unchanged.
+ * In the reference the in-place result is written out as L (tb8gen.c:1014-1017). */
+int tbg_check_successors_to(int stm, int s, void *dev_out);
+
+/* calc_sub_kslices for one slice (tb8gen.c:327-335): the five capture
+ * classes loss, bloss, draw, cwin, win of every set of colour stm, each
+ * into its own device buffer of sub_bytes, sets at sub_offset[k].  The
+ * 7-piece values come from the seeded stub (tbg_set_stub). */
+int tbg_calc_sub(int stm, int s, void *const dev_cls[5]);
+
+/* Illegal-position masks of slice s (calc_illegal_worker,
+ * tb8gen.c:734-745): for white and for black to move. */
+int tbg_calc_illegal(int s, void *dev_ill_w, void *dev_ill_b);
+
+/* Mates (L0) of slice s (calc_mate_worker, tb8gen.c:752-758). */
+int tbg_calc_mate(int s, const void *dev_ill_w, const void *dev_ill_b,
+                  void *dev_mate_w, void *dev_mate_b);
+
+/* W-step epilogue (tb8gen.c:1072-1077), fused: T(s) &= ~wins(s_wins);
+ * *cnt = popcount below the slice size; wins(s_wins) |= T(s).  s_wins is
+ * usually -1.  With cnt != NULL the call waits (bounded) for the count. */
+int tbg_epilogue_W(int s, int s_wins, uint64_t *cnt);
+
+/* Out-of-place epilogue: T(s) &= ~wins_in; wins_out = wins_in | T(s).
+ * wins_in == wins_out is tbg_epilogue_W.  The reference reads "wins" from
+ * disk into the scratch slot and writes it back (tb8gen.c:1072-1077); with
+ * HBM-resident bitmaps the old and new "wins" can be separate buffers. */
+int tbg_epilogue_W_to(int s, const void *dev_wins_in, void *dev_wins_out,
+                      uint64_t *cnt);
+
+/* kslice_count(s), kslice.c:524-527 (waits, bounded). */
+int tbg_count(int s, uint64_t *cnt);
+
+/* kslice_clear(s), kslice.c:292-296. */
+int tbg_clear(int s);
+
+/* kslice_sub_and_not(s1, s2, stm), kslice.c:481-487. */
+int tbg_sub_and_not(int s1, int s2, int stm);
+
+/* Waits (bounded: timeout_ms, 0 = 600000) for the stream; reports a kernel
+ * status word (TBG_ERR_DEVICE) if one was raised since the last wait. */
+int tbg_sync(int timeout_ms);
+
+/* Last error text (CUDA or argument detail). */
+const char *tbg_last_error(void);
+
+/* Number of kernels this library has launched so far (instrumentation). */
+int tbg_launches(uint64_t *n);
+
+/* ---- synthetic inputs (no counterpart in the reference) -------------- */
+
+/* Seeded Bernoulli bitmap: bit i < nbits set iff the (i+1)-th output of the
+ * splitmix64 stream keyed by (seed, tag) is below thr (P = thr / 2^64);
+ * the rest of the `bytes` buffer is zeroed. */
+int tbg_gen_bernoulli(void *dev, uint64_t nbits, uint64_t bytes, uint64_t seed,
+                      uint64_t tag, uint64_t thr);
+
+/* Reads n attack sets into out[] for squares sq[] and occupancies occ[]
+ * (piece type 2..6 = N, B, R, Q, K): a test hook that checks the device
+ * attack functions against movegen.h / magic.h. */
+int tbg_attacks(int type, const uint8_t *dev_sq, const uint64_t *dev_occ,
+                uint64_t *dev_out, uint64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TBGPU_H */

@@ -1,0 +1,213 @@
+"""tb8gen_b200: B200 engine for the per-king-slice ply step of tb8gen.
+
+The product is the C-ABI library ``libtbgpu.so`` (``include/tbgpu.h``), built
+in-tree from ``csrc/`` for sm_100a.  This module loads it with ctypes and
+mirrors its entry points for Python callers (tests, bench, the serving
+loop).  There is no CPU fallback: if the library is missing, importing
+``lib()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtbgpu.so")
+
+STATUS = {
+    0: "TBG_OK", -1: "TBG_ERR_ARG", -2: "TBG_ERR_STATE", -3: "TBG_ERR_UNBOUND",
+    -4: "TBG_ERR_CUDA", -5: "TBG_ERR_NOMEM", -6: "TBG_ERR_DEVICE", -7: "TBG_ERR_TIMEOUT",
+    -8: "TBG_ERR_RANGE",
+}
+
+
+class TbgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libtbgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m tb8gen_b200.build` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        vp, u64, i, sz = C.c_void_p, C.c_uint64, C.c_int, C.c_size_t
+        sig = {
+            "tbg_init": [],
+            "tbg_material_from_name": [C.c_char_p],
+            "tbg_material_select": [i],
+            "tbg_geometry": [C.POINTER(u64), C.POINTER(u64), C.POINTER(u64),
+                             C.POINTER(u64), C.POINTER(u64)],
+            "tbg_set_stream": [vp],
+            "tbg_set_stub": [u64, i],
+            "tbg_slot_bind": [i, vp, sz],
+            "tbg_sub_bind": [i, vp, sz],
+            "tbg_unbind_all": [],
+            "tbg_predecessors": [i, i],
+            "tbg_predecessors_sub": [i, i, i],
+            "tbg_check_successors": [i, i],
+            "tbg_calc_sub": [i, i, vp * 5],
+            "tbg_calc_illegal": [i, vp, vp],
+            "tbg_calc_mate": [i, vp, vp, vp, vp],
+            "tbg_epilogue_W": [i, i, C.POINTER(u64)],
+            "tbg_count": [i, C.POINTER(u64)],
+            "tbg_clear": [i],
+            "tbg_sub_and_not": [i, i, i],
+            "tbg_sync": [i],
+            "tbg_gen_bernoulli": [vp, u64, u64, u64, u64, u64],
+            "tbg_attacks": [i, vp, vp, vp, u64],
+            "tbg_check_successors_to": [i, i, vp],
+            "tbg_epilogue_W_to": [i, vp, vp, C.POINTER(u64)],
+            "tbg_launches": [C.POINTER(u64)],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.tbg_last_error.restype = C.c_char_p
+        L.tbg_last_error.argtypes = []
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> int:
+    if rc < 0:
+        raise TbgError(rc, lib().tbg_last_error().decode(errors="replace"))
+    return rc
+
+
+def ptr(t) -> C.c_void_p | None:
+    """Device address of a torch tensor (or an int address / None)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return C.c_void_p(t)
+    return C.c_void_p(t.data_ptr())
+
+
+def init(stream=None):
+    check(lib().tbg_init())
+    if stream is not None:
+        set_stream(stream)
+
+
+def set_stream(stream):
+    handle = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", 0)
+    check(lib().tbg_set_stream(C.c_void_p(handle)))
+
+
+def set_stub(seed: int, modulus: int = 3):
+    check(lib().tbg_set_stub(seed, modulus))
+
+
+class Material:
+    """A registered material (tbg_material_from_name) and its geometry."""
+
+    def __init__(self, name: str):
+        self.name = name
+        self.handle = check(lib().tbg_material_from_name(name.encode()))
+        size, nbytes, sub = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        offs, capt = (C.c_uint64 * 6)(), (C.c_uint64 * 6)()
+        check(lib().tbg_geometry(C.byref(size), C.byref(nbytes), C.byref(sub), offs, capt))
+        self.size = size.value
+        self.bytes = nbytes.value
+        self.sub_bytes = sub.value
+        self.sub_offset = list(offs)
+        self.capt_size = list(capt)
+
+    def select(self):
+        check(lib().tbg_material_select(self.handle))
+        return self
+
+
+def bind(s: int, t) -> None:
+    check(lib().tbg_slot_bind(s, ptr(t), 0 if t is None else t.numel() * t.element_size()))
+
+
+def bind_sub(s: int, t) -> None:
+    check(lib().tbg_sub_bind(s, ptr(t), 0 if t is None else t.numel() * t.element_size()))
+
+
+def unbind_all():
+    check(lib().tbg_unbind_all())
+
+
+def predecessors(stm: int, s: int):
+    check(lib().tbg_predecessors(stm, s))
+
+
+def predecessors_sub(stm: int, s: int, legality: bool):
+    check(lib().tbg_predecessors_sub(stm, s, int(bool(legality))))
+
+
+def check_successors(stm: int, s: int):
+    check(lib().tbg_check_successors(stm, s))
+
+
+def calc_sub(stm: int, s: int, cls):
+    arr = (C.c_void_p * 5)(*[t.data_ptr() for t in cls])
+    check(lib().tbg_calc_sub(stm, s, arr))
+
+
+def calc_illegal(s: int, ill_w, ill_b):
+    check(lib().tbg_calc_illegal(s, ptr(ill_w), ptr(ill_b)))
+
+
+def calc_mate(s: int, ill_w, ill_b, mate_w, mate_b):
+    check(lib().tbg_calc_mate(s, ptr(ill_w), ptr(ill_b), ptr(mate_w), ptr(mate_b)))
+
+
+def epilogue_W(s: int, s_wins: int = -1, count: bool = True):
+    c = C.c_uint64()
+    check(lib().tbg_epilogue_W(s, s_wins, C.byref(c) if count else None))
+    return c.value if count else None
+
+
+def check_successors_to(stm: int, s: int, out):
+    check(lib().tbg_check_successors_to(stm, s, ptr(out)))
+
+
+def epilogue_W_to(s: int, wins_in, wins_out, count: bool = True):
+    c = C.c_uint64()
+    check(lib().tbg_epilogue_W_to(s, ptr(wins_in), ptr(wins_out), C.byref(c) if count else None))
+    return c.value if count else None
+
+
+def launches() -> int:
+    n = C.c_uint64()
+    check(lib().tbg_launches(C.byref(n)))
+    return n.value
+
+
+def count(s: int) -> int:
+    c = C.c_uint64()
+    check(lib().tbg_count(s, C.byref(c)))
+    return c.value
+
+
+def clear(s: int):
+    check(lib().tbg_clear(s))
+
+
+def sub_and_not(s1: int, s2: int, stm: int):
+    check(lib().tbg_sub_and_not(s1, s2, stm))
+
+
+def sync(timeout_ms: int = 0):
+    check(lib().tbg_sync(timeout_ms))
+
+
+def gen_bernoulli(t, nbits: int, seed: int, tag: int, thr: int):
+    check(lib().tbg_gen_bernoulli(ptr(t), nbits, t.numel() * t.element_size(), seed, tag, thr))
+
+
+def attacks(piece_type: int, sq, occ, out):
+    check(lib().tbg_attacks(piece_type, ptr(sq), ptr(occ), ptr(out), out.numel()))

@@ -1,0 +1,71 @@
+// Host-side state of the engine: king-slice tables, materials, slot map.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "tbg_types.h"
+
+namespace tbg {
+
+// King-pair tables (probe.c:310-539, tb8gen.c:69-89) and king steps.
+struct HostTables {
+  bool ready = false;
+  int kkidx[10][64];
+  int kksq[TBG_NSLICES][2];
+  int triangle[64];
+  int flipdiag[64];
+  int mirror[64];
+  bool fliptest[64][64];
+  int kkmap[64][64];
+  uint64_t king[64];
+  void build();
+};
+
+struct Material {
+  DMat d;
+  int pt[8];
+  int num;
+  // Slot map of kslice_slot/kslice_buf/kslice_sub_buf: index s + 1, s = -1
+  // is the scratch slot.
+  uint8_t *slot[463];
+  uint64_t slot_bytes[463];
+  uint8_t *sub[463];
+  uint64_t sub_len[463];
+};
+
+struct Engine {
+  bool dev_ready = false;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  DevStatus *d_status = nullptr;
+  unsigned long long *d_cnt = nullptr;
+  unsigned long long *h_cnt = nullptr;
+  Material mats[TBG_MAX_MATS];
+  int nmats = 0;
+  int cur = -1;
+  uint64_t launches = 0;  // kernels launched by this library
+
+  int ensure_device();
+  int add_material(const int *pt, int num);
+  int fill_job(SliceJob &J, int stm, int s, bool need_sub);
+  int grid_for(uint64_t units, int per_sm);
+  int check_launch(const char *what);
+  int wait(int timeout_ms);
+};
+
+extern HostTables g_tab;
+extern Engine g_eng;
+
+int fail(int code, const char *fmt, ...);
+
+inline uint64_t tbg_host_mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace tbg
