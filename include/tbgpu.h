@@ -182,6 +182,24 @@ const char *tbg_last_error(void);
 /* Number of kernels this library has launched so far (instrumentation). */
 int tbg_launches(uint64_t *n);
 
+/* ---- epilogue without allocation (no counterpart in the reference) ---- */
+
+/* The fused W-step epilogue of tbg_epilogue_W_to on raw device pointers, for
+ * callers that cannot allocate device memory: processes whose HBM is all
+ * owned by a caching allocator or a fixed-budget pool, and foreign-language
+ * hosts whose bindings forbid a library to allocate.  It needs no tbg_init
+ * (which allocates) and calls no allocating routine; its scratch is a static
+ * 8 KiB device array held by every GPU that loads the library.
+ *   T &= ~wins_in;  wins_out = wins_in | T;  *cnt = popcount of T below nbits
+ * wins_in may equal wins_out.  `bytes` (a multiple of 16) is the bitmap size;
+ * at most 1 GiB (TBG_ERR_RANGE beyond).  The first call on a device looks up
+ * the scratch address on that device; make it before any stream capture.
+ * Calls share the scratch: calls that overlap on the GPU race and must not
+ * be issued.  Waits for the stream before returning the count. */
+int tbg_epilogue_W_static(void *dev_T, const void *dev_wins_in, void *dev_wins_out,
+                          uint64_t nbits, uint64_t bytes, void *stream,
+                          uint64_t *cnt);
+
 /* ---- synthetic inputs (no counterpart in the reference) -------------- */
 
 /* Seeded Bernoulli bitmap: bit i < nbits set iff the (i+1)-th output of the
