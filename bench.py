@@ -44,8 +44,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="slice", choices=["slice", "mix"])
-    ap.add_argument("--path", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--workload", default="slice", choices=["slice", "mix", "small"])
+    ap.add_argument("--path", default="batched", choices=["plain", "batched"])
+    ap.add_argument("--ctas-per-sm", type=int, default=0,
+                    help="persistent-kernel CTAs per SM (0: autotune)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target CPU time of the bounded CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -63,6 +65,8 @@ def dist_env():
 def workload_spec(name):
     if name == "slice":
         return [("KRRRvKRRR", 96, 0.01, 1)]
+    if name == "small":  # profiling case: 24 MB bitmaps
+        return [("KQRRvKRR", 96, 0.01, 1)]
     import numpy as np
 
     rng = np.random.default_rng(2)
@@ -170,9 +174,7 @@ def run_engine(a, rank, world, local):
     phase_names = SlicePly.PHASES
     ev = {ph: [] for ph in phase_names}
 
-    def step(timed_phases=False):
-        if a.path == "batched":
-            raise SystemExit("batched path not available in this build")
+    def direct_step(timed_phases=False):
         # phase order: all W scatters, all epilogues, all L scatters, all verifies
         for ph in phase_names:
             if timed_phases:
@@ -185,13 +187,47 @@ def run_engine(a, rank, world, local):
                 e1.record(stream)
                 ev[ph].append((e0, e1))
 
+    # the same step recorded once; mode 0 = one launch per call, 1 = persistent
+    from tb8gen_b200.plyjob import record_step
+    nops, nitems = record_step(jobs)
+    mode = 1 if a.path == "batched" else 0
+
+    def time_mode(md, reps):
+        tbg.batch_run(md)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            tbg.batch_run(md)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    # autotune the persistent launch (CTAs per SM) on this batch
+    tune = {}
+    if a.ctas_per_sm > 0:
+        tbg.batch_tune(a.ctas_per_sm)
+        best_cps = a.ctas_per_sm
+    else:
+        for cps in (1, 2, 3, 4):
+            tbg.batch_tune(cps)
+            tune[cps] = round(time_mode(1, 2), 4)
+        best_cps = min(tune, key=tune.get)
+        tbg.batch_tune(best_cps)
+
+    def step():
+        tbg.batch_run(mode)
+
+    # clocks are sampled from before the warm-up to the end of the timed steps
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
 
     # device-time throughput, inputs resident in HBM
-    clocks = ClockSampler(local)
-    clocks.start()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -213,9 +249,11 @@ def run_engine(a, rank, world, local):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
 
-    # per-phase device times (separate pass, same work)
+    # both paths on the same recorded batch, and per-phase device times
+    plain_ms = time_mode(0, max(2, a.steps // 2))
+    batched_ms = time_mode(1, max(2, a.steps // 2))
     for _ in range(max(3, a.steps // 2)):
-        step(timed_phases=True)
+        direct_step(timed_phases=True)
     torch.cuda.synchronize()
     phase_ms = {ph: statistics.median(e0.elapsed_time(e1) for e0, e1 in ev[ph])
                 for ph in phase_names}
@@ -225,15 +263,21 @@ def run_engine(a, rank, world, local):
     # end to end through the C ABI with host buffers
     e2e = None
     if not a.no_e2e:
-        e2e = run_e2e(a, jobs, stream, positions)
+        e2e = run_e2e(a, jobs, stream, positions, mode)
 
     value = positions * world / (ms / 1e3)
     peak, peak_kind = measured_peak()
-    # dominant kernel and its roofline
-    dom = max(phase_ms, key=phase_ms.get)
+    # roofline of the dominant kernel: the persistent kernel on the batched
+    # path (one launch per step), the slowest phase's kernel on the plain path
     per_pos = {"w_scatter": 0.125, "w_epilogue": 0.5, "l_scatter": 0.125, "l_verify": 0.25}
-    alg = per_pos[dom] * positions
-    achieved = alg / (phase_ms[dom] / 1e3) / 1e9
+    kname = {"w_scatter": "k_predecessors", "w_epilogue": "k_epilogue_W",
+             "l_scatter": "k_predecessors", "l_verify": "k_check_successors"}
+    if mode == 1:
+        dom, dom_ms, alg = "k_batch", ms, ALG_BYTES_PER_POS * positions
+    else:
+        ph = max(phase_ms, key=phase_ms.get)
+        dom, dom_ms, alg = kname[ph], phase_ms[ph], per_pos[ph] * positions
+    achieved = alg / (dom_ms / 1e3) / 1e9
     traffic = committed_traffic(dom)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
@@ -255,6 +299,10 @@ def run_engine(a, rank, world, local):
                    "materials": sorted({j.material for j in jobs}),
                    "l2": "inputs larger than L2 (>=16 MB bitmaps, many per step)"},
         "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+        "paths_ms": {"plain": round(plain_ms, 4), "batched": round(batched_ms, 4),
+                     "batched_speedup": round(plain_ms / batched_ms, 3)},
+        "batch": {"calls": nops, "work_items": nitems, "ctas_per_sm": best_cps,
+                  "autotune_ms": tune},
         "counts_first_jobs": counts,
         "roofline": roofline, "gpu_launches": launches, "clocks": clk,
         "e2e": e2e, "cpu_baseline": cpu,
@@ -262,31 +310,34 @@ def run_engine(a, rank, world, local):
     return line
 
 
-def run_e2e(a, jobs, stream, positions):
-    """Same steps through the C ABI with inputs in pinned host memory:
-    per step H2D of L_prev, W_prev and wins_in of every slice, the ply, and
-    D2H of W(s), L(s) and wins(s)."""
+def run_e2e(a, jobs, stream, positions, mode):
+    """Same steps through the C ABI with the sources in pinned host memory:
+    per step H2D of L_prev and W_prev of every slice, the ply (the "wins"
+    bitmaps stay resident in HBM, as the tables of a generation do), and D2H
+    of the results W(s) and L(s)."""
     import torch
+
+    import tb8gen_b200 as tbg
 
     host_in, host_out = [], []
     for j in jobs:
-        host_in.append([t.cpu().pin_memory() for t in (j.L_prev, j.W_prev, j.wins_in)])
-        host_out.append([torch.empty(j.B, dtype=torch.uint8).pin_memory() for _ in range(3)])
-    h2d = sum(j.B * 3 for j in jobs)
+        hi = [torch.empty(j.B, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+        hi[0].copy_(j.L_prev)
+        hi[1].copy_(j.W_prev)
+        host_in.append(hi)
+        host_out.append([torch.empty(j.B, dtype=torch.uint8, pin_memory=True) for _ in range(2)])
+    torch.cuda.synchronize()
+    h2d = sum(j.B * 2 for j in jobs)
     steps = max(2, min(a.steps, 5))
 
     def one():
         for j, hi in zip(jobs, host_in):
             j.L_prev.copy_(hi[0], non_blocking=True)
             j.W_prev.copy_(hi[1], non_blocking=True)
-            j.wins_in.copy_(hi[2], non_blocking=True)
-        for ph in jobs[0].PHASES:
-            for j in jobs:
-                getattr(j, ph)()
+        tbg.batch_run(mode)
         for j, ho in zip(jobs, host_out):
             ho[0].copy_(j.T, non_blocking=True)
             ho[1].copy_(j.X, non_blocking=True)
-            ho[2].copy_(j.wins, non_blocking=True)
 
     one()
     torch.cuda.synchronize()
@@ -310,7 +361,7 @@ def cpu_oracle(material, nthreads):
     return orc.Port(material), "port"
 
 
-def run_cpu_baseline(a, jobs, budget=None):
+def run_cpu_baseline(a, jobs, budget=None, inputs=None, oracle=None):
     """The reference's CPU ply (oracle/_ref, all host cores) on a bounded
     sample of the first job: sources restricted to a leading fraction of
     the slice, time extrapolated to the whole slice."""
@@ -318,8 +369,13 @@ def run_cpu_baseline(a, jobs, budget=None):
 
     budget = budget or a.cpu_seconds
     cores = os.cpu_count() or 1
-    job = jobs[0]
-    O, kind = cpu_oracle(job.material, cores)
+    job = inputs if inputs is not None else jobs[0]
+    material = job["material"] if isinstance(job, dict) else job.material
+    if oracle is None:
+        O, kind = cpu_oracle(material, cores)
+    else:
+        O, kind = oracle
+    O.set_stub(1, 3)
     threads = getattr(O, "nthreads", 1)
     frac = 0.002
     c = CpuSlicePly(O, job, frac)
@@ -335,50 +391,51 @@ def run_cpu_baseline(a, jobs, budget=None):
         scal = c.times["w_scatter"] + c.times["l_scatter"] + c.times["l_verify"]
         fixed = c.times["w_epilogue"]
     t_full = scal / frac + fixed
-    return {"value": round(job.positions / t_full, 1), "unit": UNIT, "cores": threads,
+    positions = c.N
+    return {"value": round(positions / t_full, 1), "unit": UNIT, "cores": threads,
             "kind": kind, "seconds_measured": round(t, 3),
-            "sample": (f"{job.material} slice {job.s}: scatter sources restricted to the first "
+            "sample": (f"{material} slice {c.s}: scatter sources restricted to the first "
                        f"{frac:.4f} of the slice, epilogue and verify over the whole slice; "
                        f"scatter+verify time scaled by 1/{frac:.4f}"),
             "phase_s": {k: round(v, 4) for k, v in c.times.items()}}
 
 
 def run_reference(a, rank, world, local):
-    """Reference arm: the reference's own CPU workers on the host cores."""
-    import torch
-
+    """Reference arm: the reference's own CPU workers (oracle/_ref) on all
+    host cores, inputs built on the CPU by the same workers (no engine)."""
     if rank != 0:
         return None
-    import tb8gen_b200 as tbg
-    from tb8gen_b200.plyjob import MaterialPool, SlicePly
+    from oracle.plyjob_cpu import inputs_from_oracle
 
-    # Inputs are generated by the engine's seeded generator on the GPU (the
-    # same bitmaps the engine arm uses), then copied to the host.
-    torch.cuda.set_device(local)
-    tbg.init()
+    cores = os.cpu_count() or 1
     mat, s, p, seed = workload_spec(a.workload)[0]
-    pool = MaterialPool(mat, seed) if a.workload == "mix" else None
-    job = SlicePly(mat, s, p, seed, pool)
-    torch.cuda.synchronize()
+    O, kind = cpu_oracle(mat, cores)
+    O.set_stub(1, 3)
+    t0 = time.time()
+    inputs = inputs_from_oracle(O, mat, s, p, seed)
+    prep = time.time() - t0
     per_step = []
     info = None
     for _ in range(a.warmup + a.steps):
-        info = run_cpu_baseline(a, [job], budget=min(a.cpu_seconds, 20.0))
-        per_step.append(job.positions / info["value"])
+        info = run_cpu_baseline(a, None, budget=min(a.cpu_seconds, 20.0), inputs=inputs,
+                                oracle=(O, kind))
+        per_step.append(inputs["N"] / info["value"])
     ts = per_step[a.warmup:] or per_step
     tm = statistics.median(ts)
-    v = job.positions / tm
+    v = inputs["N"] / tm
     return {
         "metric": METRIC, "value": round(v, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(tm * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded Bernoulli bitmaps, seeded 7-piece stub)",
-        "config": {"workload": a.workload, "slices": 1, "material": mat, "slice": s},
+        "config": {"workload": a.workload, "slices": 1, "material": mat, "slice": s,
+                   "note": "first slice of the workload; a step is one slice-ply"},
         "impl": "reference",
         "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": info["cores"],
                          "kind": info["kind"], "sample": info["sample"]},
         "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "input_prep_s": round(prep, 1),
     }
 
 

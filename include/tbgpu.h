@@ -172,6 +172,33 @@ int tbg_clear(int s);
 /* kslice_sub_and_not(s1, s2, stm), kslice.c:481-487. */
 int tbg_sub_and_not(int s1, int s2, int stm);
 
+/* ---- batched ply (persistent kernel) ---------------------------------- */
+
+/* Starts recording: the following ply-step calls (tbg_predecessors,
+ * tbg_predecessors_sub, tbg_check_successors[_to], tbg_epilogue_W[_to] with
+ * cnt == NULL, tbg_clear) are checked and recorded with their current
+ * bindings instead of launched.  No counterpart in the reference, whose
+ * schedule runs one run_threaded call at a time (threads.c:266-289). */
+int tbg_batch_begin(void);
+
+/* Ends recording and uploads the batch (the library allocates its work
+ * queue here).  Reports the number of recorded calls and of work items. */
+int tbg_batch_end(int *nops, uint64_t *nitems);
+
+/* Runs the recorded batch on the current stream: mode 0 launches one kernel
+ * per recorded call in record order (the plain path); mode 1 runs all of
+ * them in one persistent kernel fed by a device work queue, each call
+ * starting tile by tile as soon as the calls it depends on (by buffer) are
+ * done.  Both give the same bitmaps as the calls made one by one. */
+int tbg_batch_run(int mode);
+
+/* Epilogue counts of the last run, in record order (waits, bounded). */
+int tbg_batch_counts(uint64_t *out, int n);
+
+/* Persistent-launch configuration: CTAs per SM, and the iteration bound of
+ * a dependency wait (<= 0 keeps the current one). */
+int tbg_batch_tune(int ctas_per_sm, long long spin_limit);
+
 /* Waits (bounded: timeout_ms, 0 = 600000) for the stream; reports a kernel
  * status word (TBG_ERR_DEVICE) if one was raised since the last wait. */
 int tbg_sync(int timeout_ms);

@@ -29,32 +29,78 @@ def _sample(a: np.ndarray, nbits: int, frac: float) -> np.ndarray:
     return out
 
 
+def inputs_from_engine_job(job) -> dict:
+    """Host copies of an engine job's inputs (tb8gen_b200.plyjob.SlicePly)."""
+    h = lambda t: t.cpu().numpy().copy()
+    d = {"material": job.material, "s": job.s, "N": job.N, "B": job.B,
+         "L_prev": h(job.L_prev), "W_prev": h(job.W_prev), "wins_in": h(job.wins_in),
+         "sub_win": h(job.sub_win), "wk": list(job.wk), "bk": list(job.bk),
+         "shared": job.pool is not None}
+    if job.pool is not None:
+        d["wins_nbr"] = {t: None for t in job.bk}
+        d["pool_wins"], d["pool_sub"] = h(job.pool.wins_nbr), h(job.pool.sub_nbr)
+        d["sub_nbr"] = {t: None for t in job.bk}
+    else:
+        d["wins_nbr"] = {t: h(job.wins_nbr[t]) for t in job.bk}
+        d["sub_nbr"] = {t: h(job.sub_nbr[t]) for t in job.bk}
+    return d
+
+
+def inputs_from_oracle(O, material: str, s: int, p: float, seed: int) -> dict:
+    """The same inputs as tb8gen_b200.plyjob.SlicePly(material, s, p, seed)
+    (no shared neighbours), computed on the CPU by the oracle O itself: the
+    illegal masks and sub/win bitmaps by its calc_illegal / calc_sub, the
+    Bernoulli sources by the same seeded splitmix64 stream."""
+    from oracle.oracle import bitmap_tag, gen_bitmap, king_targets
+
+    N, B = O.size, O.bytes
+
+    def illegal(t):
+        w, b = np.zeros(B, np.uint8), np.zeros(B, np.uint8)
+        O.calc_illegal(t, w, b)
+        return w, b
+
+    def sub_win(t):
+        cls = [np.zeros(O.sub_bytes, np.uint8) for _ in range(5)]
+        O.calc_sub(WHITE, t, cls)
+        return cls[4]
+
+    ill_w, ill_b = illegal(s)
+    d = {"material": material, "s": s, "N": N, "B": B,
+         "L_prev": gen_bitmap(N, B, seed, bitmap_tag(0, BLACK, s), p) & ~ill_b,
+         "W_prev": gen_bitmap(N, B, seed, bitmap_tag(3, WHITE, s), p) & ~ill_w,
+         "wins_in": ill_w, "sub_win": sub_win(s),
+         "wk": king_targets(WHITE, s), "bk": king_targets(BLACK, s), "shared": False}
+    d["wins_nbr"] = {t: illegal(t)[0] for t in d["bk"]}
+    d["sub_nbr"] = {t: sub_win(t) for t in d["bk"]}
+    return d
+
+
 class CpuSlicePly:
     def __init__(self, O, job, frac: float = 1.0):
-        """O: oracle.Ref or oracle.Port for job.material; job: a SlicePly
-        whose device inputs are copied to the host."""
-        self.O, self.s, self.frac = O, job.s, frac
-        self.N, self.B = job.N, job.B
-        h = lambda t: t.cpu().numpy().copy()
-        self.L_prev = _sample(h(job.L_prev), self.N, frac)
-        self.W_prev = _sample(h(job.W_prev), self.N, frac)
-        self.wins_in = h(job.wins_in)
-        self.sub_win = h(job.sub_win)
-        self.wk, self.bk = list(job.wk), list(job.bk)
-        self.shared = job.pool is not None
-        # neighbour buffers, shared or not exactly as on the device
+        """O: oracle.Ref or oracle.Port for the job's material; job: an
+        engine SlicePly (its inputs are copied to the host) or a dict from
+        inputs_from_oracle / inputs_from_engine_job."""
+        d = job if isinstance(job, dict) else inputs_from_engine_job(job)
+        self.O, self.s, self.frac = O, d["s"], frac
+        self.N, self.B = d["N"], d["B"]
+        self.L_prev = _sample(d["L_prev"], self.N, frac)
+        self.W_prev = _sample(d["W_prev"], self.N, frac)
+        self.wins_in = d["wins_in"]
+        self.sub_win = d["sub_win"]
+        self.wk, self.bk = list(d["wk"]), list(d["bk"])
+        self.shared = d["shared"]
         if self.shared:
             ts, xs = np.zeros(self.B, np.uint8), np.zeros(self.B, np.uint8)
-            wn, sn = h(job.pool.wins_nbr), h(job.pool.sub_nbr)
             self.T_nbr = {t: ts for t in self.wk}
             self.X_nbr = {t: xs for t in self.bk}
-            self.wins_nbr = {t: wn for t in self.bk}
-            self.sub_nbr = {t: sn for t in self.bk}
+            self.wins_nbr = {t: d["pool_wins"] for t in self.bk}
+            self.sub_nbr = {t: d["pool_sub"] for t in self.bk}
         else:
             self.T_nbr = {t: np.zeros(self.B, np.uint8) for t in self.wk}
             self.X_nbr = {t: np.zeros(self.B, np.uint8) for t in self.bk}
-            self.wins_nbr = {t: h(job.wins_nbr[t]) for t in self.bk}
-            self.sub_nbr = {t: h(job.sub_nbr[t]) for t in self.bk}
+            self.wins_nbr = dict(d["wins_nbr"])
+            self.sub_nbr = dict(d["sub_nbr"])
         self.T = np.zeros(self.B, np.uint8)
         self.X = np.zeros(self.B, np.uint8)
         self.wins = np.zeros(self.B, np.uint8)

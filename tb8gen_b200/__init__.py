@@ -12,7 +12,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libtbgpu.so")
+# TBGPU_LIB selects another build of the library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("TBGPU_LIB") or os.path.join(HERE, "libtbgpu.so")
 
 STATUS = {
     0: "TBG_OK", -1: "TBG_ERR_ARG", -2: "TBG_ERR_STATE", -3: "TBG_ERR_UNBOUND",
@@ -67,6 +68,11 @@ def lib():
             "tbg_check_successors_to": [i, i, vp],
             "tbg_epilogue_W_to": [i, vp, vp, C.POINTER(u64)],
             "tbg_launches": [C.POINTER(u64)],
+            "tbg_batch_begin": [],
+            "tbg_batch_end": [C.POINTER(i), C.POINTER(u64)],
+            "tbg_batch_run": [i],
+            "tbg_batch_counts": [C.POINTER(u64), i],
+            "tbg_batch_tune": [i, C.c_longlong],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -211,3 +217,28 @@ def gen_bernoulli(t, nbits: int, seed: int, tag: int, thr: int):
 
 def attacks(piece_type: int, sq, occ, out):
     check(lib().tbg_attacks(piece_type, ptr(sq), ptr(occ), ptr(out), out.numel()))
+
+
+def batch_begin():
+    check(lib().tbg_batch_begin())
+
+
+def batch_end():
+    n, items = C.c_int(), C.c_uint64()
+    check(lib().tbg_batch_end(C.byref(n), C.byref(items)))
+    return n.value, items.value
+
+
+def batch_run(mode: int):
+    """mode 0: one launch per recorded call; mode 1: one persistent launch."""
+    check(lib().tbg_batch_run(mode))
+
+
+def batch_counts(n: int):
+    out = (C.c_uint64 * max(n, 1))()
+    check(lib().tbg_batch_counts(out, n))
+    return list(out)[:n]
+
+
+def batch_tune(ctas_per_sm: int, spin_limit: int = 0):
+    check(lib().tbg_batch_tune(ctas_per_sm, spin_limit))

@@ -10,7 +10,7 @@
 
 #include "../../include/tbgpu.h"
 #include "tbg_host.h"
-#include "tbg_kernels.cuh"
+#include "tbg_batch.cuh"
 
 namespace tbg {
 
@@ -36,6 +36,24 @@ int cuda_fail(cudaError_t e, const char *what) {
     cudaError_t e_ = (call);                       \
     if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
   } while (0)
+
+// Kernels are compiled for each number of piece sets (1..6); NS_SWITCH picks
+// the instance of the current material.
+#define NS_CASE(n, ...) \
+  case n: {             \
+    constexpr int NS = n; \
+    __VA_ARGS__;        \
+  } break;
+#define NS_SWITCH(ns, ...)                                                   \
+  switch (ns) {                                                              \
+    NS_CASE(1, __VA_ARGS__)                                                  \
+    NS_CASE(2, __VA_ARGS__)                                                  \
+    NS_CASE(3, __VA_ARGS__)                                                  \
+    NS_CASE(4, __VA_ARGS__)                                                  \
+    NS_CASE(5, __VA_ARGS__)                                                  \
+    NS_CASE(6, __VA_ARGS__)                                                  \
+    default: return fail(TBG_ERR_RANGE, "%d piece sets", (int)(ns));         \
+  }
 
 // ------------------------------------------------------------ host tables
 // The king-pair tables of probe.c:441-539 and tb8gen.c:69-89, generated from
@@ -437,78 +455,114 @@ extern "C" int tbg_unbind_all(void) {
   return TBG_OK;
 }
 
+// ---------------------------------------------------------------- ops
+// Every call of the ply step becomes an Op; outside a recording it is
+// launched at once, inside one it is appended to the batch.
+static uint32_t op_tiles(const Op &o) {
+  if (o.kind == OP_EPILOGUE || o.kind == OP_CLEAR) return (uint32_t)((o.n16 + kChunk16 - 1) / kChunk16);
+  return (uint32_t)((o.J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull));
+}
+
+static int launch_op(const Op &o) {
+  const int ns = o.ns;
+  cudaStream_t st = g_eng.stream;
+  switch (o.kind) {
+  case OP_SCATTER:
+    NS_SWITCH(ns, k_predecessors<NS><<<g_eng.grid_for(o.ntiles, g_eng.bps_scatter), kThreads, 0, st>>>(
+                      o.J, g_eng.d_status));
+    return g_eng.check_launch("k_predecessors");
+  case OP_SCATTER_SUB:
+    NS_SWITCH(ns, k_predecessors_sub<NS><<<g_eng.grid_for(o.ntiles, g_eng.bps_scatter), kThreads, 0,
+                                           st>>>(o.J, g_eng.d_status));
+    return g_eng.check_launch("k_predecessors_sub");
+  case OP_VERIFY:
+    NS_SWITCH(ns, k_check_successors<NS><<<g_eng.grid_for(o.ntiles, g_eng.bps_verify), kThreads, 0,
+                                           st>>>(o.J, g_eng.d_status, o.out, o.out_words));
+    return g_eng.check_launch("k_check_successors");
+  case OP_EPILOGUE: {
+    uint64_t n16 = o.n16;
+    k_epilogue_W<<<g_eng.grid_for((n16 + kThreads - 1) / kThreads, 8), kThreads, 0, st>>>(
+        o.T, o.win, o.wout, n16, o.nbits, o.cnt);
+    return g_eng.check_launch("k_epilogue_W");
+  }
+  case OP_CLEAR:
+    CK(cudaMemsetAsync(o.T, 0, o.n16 * 16, st));
+    return TBG_OK;
+  }
+  return fail(TBG_ERR_ARG, "unknown op");
+}
+
+static int submit(Op &o) {
+  o.ntiles = op_tiles(o);
+  if (g_eng.batch.recording) return g_eng.batch.add(o);
+  return launch_op(o);
+}
+
+static Op new_op(int kind) {
+  Op o;
+  memset(&o, 0, sizeof o);
+  o.kind = kind;
+  o.cnt_slot = -1;
+  o.ns = g_eng.mats[g_eng.cur].d.ii.numsets;
+  return o;
+}
+
 extern "C" int tbg_predecessors(int stm, int s) {
   NEED_MAT();
   if ((stm & ~1) || s < 0 || s >= TBG_NSLICES) return fail(TBG_ERR_ARG, "bad stm/slice");
   Material &m = g_eng.mats[g_eng.cur];
-  SliceJob J;
-  int rc = g_eng.fill_job(J, stm, s, false);
+  Op o = new_op(OP_SCATTER);
+  int rc = g_eng.fill_job(o.J, stm, s, false);
   if (rc) return rc;
   if (!m.slot[0]) return fail(TBG_ERR_UNBOUND, "scratch slot not bound");
-  J.src = reinterpret_cast<const uint32_t *>(m.slot[0]);
-  J.cand = nullptr;
-  J.nbits = m.d.ii.size;
-  uint64_t tiles = (J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull);
-  k_predecessors<<<g_eng.grid_for(tiles, 8), kThreads, 0, g_eng.stream>>>(J, g_eng.d_status);
-  return g_eng.check_launch("k_predecessors");
+  o.J.src = reinterpret_cast<const uint32_t *>(m.slot[0]);
+  o.J.cand = nullptr;
+  o.J.nbits = m.d.ii.size;
+  return submit(o);
 }
 
 extern "C" int tbg_predecessors_sub(int stm, int s, int legality) {
   NEED_MAT();
   if ((stm & ~1) || s < 0 || s >= TBG_NSLICES) return fail(TBG_ERR_ARG, "bad stm/slice");
   Material &m = g_eng.mats[g_eng.cur];
-  SliceJob J;
-  int rc = g_eng.fill_job(J, stm, s, false);
+  Op o = new_op(OP_SCATTER_SUB);
+  int rc = g_eng.fill_job(o.J, stm, s, false);
   if (rc) return rc;
-  if (!J.self_sub) return fail(TBG_ERR_UNBOUND, "sub of slice %d not bound", s);
-  J.legality = legality != 0;
-  J.cand = nullptr;
+  if (!o.J.self_sub) return fail(TBG_ERR_UNBOUND, "sub of slice %d not bound", s);
+  o.J.legality = legality != 0;
+  o.J.cand = nullptr;
   for (int k = 0; k < m.d.ii.numsets; k++) {
     if (m.d.set_color[k] == stm) continue;
-    J.set = k;
-    J.src = reinterpret_cast<const uint32_t *>(J.self_sub + m.d.sub_offset[k]);
-    J.nbits = m.d.capt[k].size;
-    uint64_t tiles = (J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull);
-    k_predecessors_sub<<<g_eng.grid_for(tiles, 8), kThreads, 0, g_eng.stream>>>(J, g_eng.d_status);
-    rc = g_eng.check_launch("k_predecessors_sub");
+    o.J.set = k;
+    o.J.src = reinterpret_cast<const uint32_t *>(o.J.self_sub + m.d.sub_offset[k]);
+    o.J.nbits = m.d.capt[k].size;
+    rc = submit(o);
     if (rc) return rc;
   }
   return TBG_OK;
 }
 
-extern "C" int tbg_check_successors(int stm, int s) {
+static int check_successors(int stm, int s, uint32_t *out) {
   NEED_MAT();
   if ((stm & ~1) || s < 0 || s >= TBG_NSLICES) return fail(TBG_ERR_ARG, "bad stm/slice");
   Material &m = g_eng.mats[g_eng.cur];
-  SliceJob J;
-  int rc = g_eng.fill_job(J, stm, s, true);
+  Op o = new_op(OP_VERIFY);
+  int rc = g_eng.fill_job(o.J, stm, s, true);
   if (rc) return rc;
   if (!m.slot[0]) return fail(TBG_ERR_UNBOUND, "scratch slot not bound");
-  J.cand = reinterpret_cast<uint32_t *>(m.slot[0]);
-  J.src = J.cand;
-  J.nbits = m.d.ii.size;
-  uint64_t tiles = (J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull);
-  k_check_successors<<<g_eng.grid_for(tiles, 8), kThreads, 0, g_eng.stream>>>(
-      J, g_eng.d_status, nullptr, 0);
-  return g_eng.check_launch("k_check_successors");
+  o.J.cand = reinterpret_cast<uint32_t *>(m.slot[0]);
+  o.J.src = o.J.cand;
+  o.J.nbits = m.d.ii.size;
+  o.out = out;
+  o.out_words = out ? m.d.bytes / 4 : 0;
+  return submit(o);
 }
 
+extern "C" int tbg_check_successors(int stm, int s) { return check_successors(stm, s, nullptr); }
+
 extern "C" int tbg_check_successors_to(int stm, int s, void *dev_out) {
-  NEED_MAT();
-  if ((stm & ~1) || s < 0 || s >= TBG_NSLICES || !dev_out || !aligned16(dev_out))
-    return fail(TBG_ERR_ARG, "bad stm/slice/output");
-  Material &m = g_eng.mats[g_eng.cur];
-  SliceJob J;
-  int rc = g_eng.fill_job(J, stm, s, true);
-  if (rc) return rc;
-  if (!m.slot[0]) return fail(TBG_ERR_UNBOUND, "scratch slot not bound");
-  J.cand = reinterpret_cast<uint32_t *>(m.slot[0]);
-  J.src = J.cand;
-  J.nbits = m.d.ii.size;
-  uint64_t tiles = (J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull);
-  k_check_successors<<<g_eng.grid_for(tiles, 8), kThreads, 0, g_eng.stream>>>(
-      J, g_eng.d_status, static_cast<uint32_t *>(dev_out), m.d.bytes / 4);
-  return g_eng.check_launch("k_check_successors");
+  if (!dev_out || !aligned16(dev_out)) return fail(TBG_ERR_ARG, "bad output");
+  return check_successors(stm, s, static_cast<uint32_t *>(dev_out));
 }
 
 extern "C" int tbg_calc_sub(int stm, int s, void *const dev_cls[5]) {
@@ -531,8 +585,8 @@ extern "C" int tbg_calc_sub(int stm, int s, void *const dev_cls[5]) {
     uint64_t nwords = (m.d.capt[k].size + 31) / 32;
     uint32_t *c[5];
     for (int i = 0; i < 5; i++) c[i] = reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(dev_cls[i]) + off);
-    k_calc_sub<<<g_eng.grid_for((nwords + kThreads - 1) / kThreads, 16), kThreads, 0,
-                 g_eng.stream>>>(J, c[0], c[1], c[2], c[3], c[4]);
+    NS_SWITCH(m.d.ii.numsets, k_calc_sub<NS><<<g_eng.grid_for((nwords + kThreads - 1) / kThreads, 16), kThreads, 0,
+                 g_eng.stream>>>(J, c[0], c[1], c[2], c[3], c[4]));
     int rc = g_eng.check_launch("k_calc_sub");
     if (rc) return rc;
   }
@@ -552,9 +606,9 @@ extern "C" int tbg_calc_illegal(int s, void *dev_ill_w, void *dev_ill_b) {
   J.k0 = g_tab.kksq[s][0];
   J.k1 = g_tab.kksq[s][1];
   uint64_t nwords = m.d.bytes / 4;
-  k_calc_illegal<<<g_eng.grid_for((nwords + kThreads - 1) / kThreads, 16), kThreads, 0,
+  NS_SWITCH(m.d.ii.numsets, k_calc_illegal<NS><<<g_eng.grid_for((nwords + kThreads - 1) / kThreads, 16), kThreads, 0,
                    g_eng.stream>>>(J, static_cast<uint32_t *>(dev_ill_w),
-                                   static_cast<uint32_t *>(dev_ill_b), nwords);
+                                   static_cast<uint32_t *>(dev_ill_b), nwords));
   return g_eng.check_launch("k_calc_illegal");
 }
 
@@ -571,22 +625,31 @@ extern "C" int tbg_calc_mate(int s, const void *dev_ill_w, const void *dev_ill_b
   J.k0 = g_tab.kksq[s][0];
   J.k1 = g_tab.kksq[s][1];
   uint64_t nwords = m.d.bytes / 4;
-  k_calc_mate<<<g_eng.grid_for((nwords + kThreads - 1) / kThreads, 16), kThreads, 0,
+  NS_SWITCH(m.d.ii.numsets, k_calc_mate<NS><<<g_eng.grid_for((nwords + kThreads - 1) / kThreads, 16), kThreads, 0,
                 g_eng.stream>>>(J, static_cast<const uint32_t *>(dev_ill_w),
                                 static_cast<const uint32_t *>(dev_ill_b),
                                 static_cast<uint32_t *>(dev_mate_w),
-                                static_cast<uint32_t *>(dev_mate_b), nwords);
+                                static_cast<uint32_t *>(dev_mate_b), nwords));
   return g_eng.check_launch("k_calc_mate");
 }
 
 static int epilogue(uint8_t *T, const uint8_t *Win, uint8_t *Wout, uint64_t *cnt) {
   Material &m = g_eng.mats[g_eng.cur];
+  Op o = new_op(OP_EPILOGUE);
+  o.T = reinterpret_cast<uint4 *>(T);
+  o.win = reinterpret_cast<const uint4 *>(Win);
+  o.wout = reinterpret_cast<uint4 *>(Wout);
+  o.n16 = m.d.bytes / 16;
+  o.nbits = m.d.ii.size;
+  if (g_eng.batch.recording) {
+    if (cnt) return fail(TBG_ERR_STATE, "counts of a recorded epilogue come from tbg_batch_counts");
+    o.cnt_slot = g_eng.batch.ncounts++;
+    o.cnt = nullptr;
+    return submit(o);
+  }
   CK(cudaMemsetAsync(g_eng.d_cnt, 0, sizeof(unsigned long long), g_eng.stream));
-  uint64_t n16 = m.d.bytes / 16;
-  k_epilogue_W<<<g_eng.grid_for((n16 + kThreads - 1) / kThreads, 8), kThreads, 0, g_eng.stream>>>(
-      reinterpret_cast<uint4 *>(T), reinterpret_cast<const uint4 *>(Win),
-      reinterpret_cast<uint4 *>(Wout), n16, m.d.ii.size, g_eng.d_cnt);
-  int rc = g_eng.check_launch("k_epilogue_W");
+  o.cnt = g_eng.d_cnt;
+  int rc = submit(o);
   if (rc || !cnt) return rc;
   CK(cudaMemcpyAsync(g_eng.h_cnt, g_eng.d_cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                      g_eng.stream));
@@ -644,8 +707,10 @@ extern "C" int tbg_clear(int s) {
   if (s < -1 || s >= TBG_NSLICES) return fail(TBG_ERR_ARG, "bad slice");
   Material &m = g_eng.mats[g_eng.cur];
   if (!m.slot[s + 1]) return fail(TBG_ERR_UNBOUND, "slice %d not bound", s);
-  CK(cudaMemsetAsync(m.slot[s + 1], 0, m.d.bytes, g_eng.stream));
-  return TBG_OK;
+  Op o = new_op(OP_CLEAR);
+  o.T = reinterpret_cast<uint4 *>(m.slot[s + 1]);
+  o.n16 = m.d.bytes / 16;
+  return submit(o);
 }
 
 extern "C" int tbg_sub_and_not(int s1, int s2, int stm) {
@@ -704,5 +769,182 @@ extern "C" int tbg_attacks(int type, const uint8_t *dev_sq, const uint64_t *dev_
 extern "C" int tbg_launches(uint64_t *n) {
   if (!n) return fail(TBG_ERR_ARG, "null");
   *n = g_eng.launches;
+  return TBG_OK;
+}
+
+// ------------------------------------------------------------- batches
+namespace tbg {
+
+void Batch::clear() {
+  ops.clear();
+  acc.clear();
+  preds.clear();
+  ncounts = 0;
+  nsmax = 1;
+  total = 0;
+  ready = false;
+}
+
+static void access_of(const Op &o, Batch::Access &a) {
+  const SliceJob &J = o.J;
+  switch (o.kind) {
+  case OP_SCATTER:
+    a.rd.push_back(J.src);
+    a.wacc.push_back(J.self);
+    for (int d = 0; d < J.nk; d++) a.wacc.push_back(J.kd[d].bits);
+    break;
+  case OP_SCATTER_SUB:
+    a.rd.push_back(J.self_sub);
+    a.wacc.push_back(J.self);
+    for (int d = 0; d < J.nk; d++) a.wacc.push_back(J.kd[d].bits);
+    break;
+  case OP_VERIFY:
+    a.rd.push_back(J.cand);
+    a.rd.push_back(J.self);
+    a.rd.push_back(J.self_sub);
+    for (int d = 0; d < J.nk; d++) {
+      a.rd.push_back(J.kd[d].bits);
+      a.rd.push_back(J.kd[d].sub);
+    }
+    a.wplain.push_back(o.out ? static_cast<const void *>(o.out) : J.cand);
+    break;
+  case OP_EPILOGUE:
+    a.rd.push_back(o.T);
+    a.rd.push_back(o.win);
+    a.wplain.push_back(o.T);
+    a.wplain.push_back(o.wout);
+    break;
+  case OP_CLEAR:
+    a.wplain.push_back(o.T);
+    break;
+  }
+}
+
+static bool contains(const std::vector<const void *> &v, const void *p) {
+  return p != nullptr && std::find(v.begin(), v.end(), p) != v.end();
+}
+
+// Whether op b (recorded after a) must wait for a: a write of one meets a
+// read or write of the other; two accumulating scatters commute.
+static bool conflicts(const Batch::Access &a, const Batch::Access &b) {
+  for (const void *x : a.wplain)
+    if (contains(b.rd, x) || contains(b.wplain, x) || contains(b.wacc, x)) return true;
+  for (const void *x : a.wacc)
+    if (contains(b.rd, x) || contains(b.wplain, x)) return true;
+  for (const void *x : a.rd)
+    if (contains(b.wplain, x) || contains(b.wacc, x)) return true;
+  return false;
+}
+
+int Batch::add(Op &o) {
+  Access a;
+  access_of(o, a);
+  o.pred_off = (int)preds.size();
+  o.npred = 0;
+  for (size_t i = 0; i < ops.size(); i++)
+    if (conflicts(acc[i], a)) {
+      preds.push_back((int)i);
+      o.npred++;
+    }
+  if (o.kind != OP_EPILOGUE && o.kind != OP_CLEAR) nsmax = std::max(nsmax, o.ns);
+  o.first = total;
+  total += o.ntiles;
+  ops.push_back(o);
+  acc.push_back(std::move(a));
+  return TBG_OK;
+}
+
+template <class T>
+static int grow(T **p, size_t *cap, size_t n) {
+  if (n <= *cap) return TBG_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  size_t c = std::max(n, (size_t)64);
+  cudaError_t e = cudaMalloc(p, c * sizeof(T));
+  if (e != cudaSuccess) return fail(TBG_ERR_NOMEM, "batch queue: %s", cudaGetErrorString(e));
+  *cap = c;
+  return TBG_OK;
+}
+
+int Batch::finish() {
+  int rc;
+  if ((rc = grow(&d_ops, &cap_ops, ops.size()))) return rc;
+  if ((rc = grow(&d_preds, &cap_preds, std::max<size_t>(preds.size(), 1)))) return rc;
+  if ((rc = grow(&d_done, &cap_done, ops.size()))) return rc;
+  if ((rc = grow(&d_counts, &cap_counts, std::max(ncounts, 1)))) return rc;
+  if (!d_next) {
+    cudaError_t e = cudaMalloc(&d_next, sizeof(unsigned long long));
+    if (e != cudaSuccess) return fail(TBG_ERR_NOMEM, "batch queue: %s", cudaGetErrorString(e));
+  }
+  for (Op &o : ops) o.cnt = o.cnt_slot >= 0 ? d_counts + o.cnt_slot : nullptr;
+  CK(cudaMemcpy(d_ops, ops.data(), ops.size() * sizeof(Op), cudaMemcpyHostToDevice));
+  if (!preds.empty())
+    CK(cudaMemcpy(d_preds, preds.data(), preds.size() * sizeof(int), cudaMemcpyHostToDevice));
+  ready = true;
+  return TBG_OK;
+}
+
+}  // namespace tbg
+
+extern "C" int tbg_batch_begin(void) {
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  if (g_eng.batch.recording) return fail(TBG_ERR_STATE, "already recording");
+  g_eng.batch.clear();
+  g_eng.batch.recording = true;
+  return TBG_OK;
+}
+
+extern "C" int tbg_batch_end(int *nops, uint64_t *nitems) {
+  Batch &b = g_eng.batch;
+  if (!b.recording) return fail(TBG_ERR_STATE, "not recording");
+  b.recording = false;
+  if (b.ops.empty()) return fail(TBG_ERR_ARG, "empty batch");
+  int rc = b.finish();
+  if (rc) return rc;
+  if (nops) *nops = (int)b.ops.size();
+  if (nitems) *nitems = b.total;
+  return TBG_OK;
+}
+
+extern "C" int tbg_batch_tune(int ctas_per_sm, long long spin_limit) {
+  if (ctas_per_sm < 1 || ctas_per_sm > 32) return fail(TBG_ERR_ARG, "ctas_per_sm 1..32");
+  g_eng.batch.ctas_per_sm = ctas_per_sm;
+  if (spin_limit > 0) g_eng.batch.spin_limit = spin_limit;
+  return TBG_OK;
+}
+
+extern "C" int tbg_batch_run(int mode) {
+  Batch &b = g_eng.batch;
+  if (!b.ready) return fail(TBG_ERR_STATE, "no recorded batch");
+  cudaStream_t st = g_eng.stream;
+  CK(cudaMemsetAsync(b.d_counts, 0, std::max(b.ncounts, 1) * sizeof(unsigned long long), st));
+  if (mode == 0) {
+    for (const Op &o : b.ops) {
+      int rc = launch_op(o);
+      if (rc) return rc;
+    }
+    return TBG_OK;
+  }
+  if (mode != 1) return fail(TBG_ERR_ARG, "mode 0 (one launch per call) or 1 (persistent)");
+  CK(cudaMemsetAsync(b.d_done, 0, b.ops.size() * sizeof(unsigned int), st));
+  CK(cudaMemsetAsync(b.d_next, 0, sizeof(unsigned long long), st));
+  int grid = g_eng.num_sms * b.ctas_per_sm;
+  if (b.nsmax <= 3)
+    k_batch<3><<<grid, kThreads, 0, st>>>(b.d_ops, (int)b.ops.size(), b.d_preds, b.total, b.d_next,
+                                          b.d_done, g_eng.d_status, b.spin_limit);
+  else
+    k_batch<6><<<grid, kThreads, 0, st>>>(b.d_ops, (int)b.ops.size(), b.d_preds, b.total, b.d_next,
+                                          b.d_done, g_eng.d_status, b.spin_limit);
+  return g_eng.check_launch("k_batch");
+}
+
+extern "C" int tbg_batch_counts(uint64_t *out, int n) {
+  Batch &b = g_eng.batch;
+  if (!b.ready || !out || n < 0 || n > b.ncounts) return fail(TBG_ERR_ARG, "bad count request");
+  if (n == 0) return TBG_OK;
+  int rc = g_eng.wait(0);
+  if (rc) return rc;
+  CK(cudaMemcpy(out, b.d_counts, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   return TBG_OK;
 }

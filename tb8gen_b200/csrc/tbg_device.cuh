@@ -138,13 +138,14 @@ __device__ __forceinline__ uint32_t fast_div32(uint32_t n, uint64_t M) {
 // Combinatorial rank of the sets of a position (sq_to_idx_helper,
 // tb8gen.c:129-149): each set's squares, in increasing order, ranked among
 // the squares not taken by the kings and earlier sets.
+template <int NS>
 __device__ __forceinline__ uint64_t rank_sets(const DIdx &X, const uint32_t *bin,
                                              int k0, int k1, const bb *set) {
   bb occ = bit(k0) | bit(k1);
   uint64_t idx = 0;
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) {
-    if (k < X.numsets) {
+  for (int k = 0; k < NS; k++) {
+    {
       bb b = set[k];
       uint32_t s = 0;
       int j = 1;
@@ -171,15 +172,16 @@ __device__ __forceinline__ int nth_set(bb b, int r) {
 
 // Inverse of rank_sets (idx_to_sq_init + unrank_binomial, tb8gen.c:105-126,
 // 169-175): fills set[] and returns the occupancy, kings included.
+template <int NS>
 __device__ __forceinline__ bb unrank_sets(const DIdx &X, const uint32_t *bin,
                                          uint64_t idx, int k0, int k1, bb *set) {
   bb occ = bit(k0) | bit(k1);
   uint32_t rem32 = (uint32_t)idx;
   bool small = idx < (1ull << 32);
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) {
+  for (int k = 0; k < NS; k++) {
     set[k] = 0;
-    if (k < X.numsets) {
+    {
       uint32_t d;
       if (small) {
         d = fast_div32(rem32, X.fdiv[k]);
@@ -217,12 +219,13 @@ __device__ __forceinline__ bb unrank_sets(const DIdx &X, const uint32_t *bin,
 // Whether a piece of colour `color` attacks square `target` (is_attacked_by,
 // movegen.h:180-188), given each set's type/colour, the king squares and
 // the occupancy.
+template <int NS>
 __device__ __forceinline__ bool attacked_by(const DMat &M, const bb *set, int k0, int k1,
                                             bb occ, int target, int color) {
   bb rq = 0, bq = 0, n = 0;
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) {
-    if (k < M.ii.numsets && M.set_color[k] == color) {
+  for (int k = 0; k < NS; k++) {
+    if (M.set_color[k] == color) {
       int t = M.set_type[k];
       if (t == 4 || t == 5) rq |= set[k];
       if (t == 3 || t == 5) bq |= set[k];

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <vector>
 
 #include "tbg_types.h"
 
@@ -36,6 +37,39 @@ struct Material {
   uint64_t sub_len[463];
 };
 
+
+// A recorded batch of ply-step calls (tbg_batch_begin .. tbg_batch_end).
+struct Batch {
+  bool recording = false;
+  bool ready = false;
+  std::vector<Op> ops;
+  struct Access {
+    std::vector<const void *> rd, wplain, wacc;
+  };
+  std::vector<Access> acc;
+  std::vector<int> preds;
+  int ncounts = 0;
+  int nsmax = 1;
+  uint64_t total = 0;
+  // device copies
+  Op *d_ops = nullptr;
+  size_t cap_ops = 0;
+  int *d_preds = nullptr;
+  size_t cap_preds = 0;
+  unsigned int *d_done = nullptr;
+  size_t cap_done = 0;
+  unsigned long long *d_counts = nullptr;
+  size_t cap_counts = 0;
+  unsigned long long *d_next = nullptr;
+  // persistent launch configuration
+  int ctas_per_sm = 2;
+  long long spin_limit = 50000000;
+
+  void clear();
+  int add(Op &o);
+  int finish();
+};
+
 struct Engine {
   bool dev_ready = false;
   int device = 0;
@@ -48,6 +82,9 @@ struct Engine {
   int nmats = 0;
   int cur = -1;
   uint64_t launches = 0;  // kernels launched by this library
+  int bps_scatter = 8;    // grid = SMs x this for the sparse kernels (tiles loop)
+  int bps_verify = 8;
+  Batch batch;
 
   int ensure_device();
   int add_material(const int *pt, int num);

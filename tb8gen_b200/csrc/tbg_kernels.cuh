@@ -20,6 +20,14 @@
 
 namespace tbg {
 
+// Blocks per SM the sparse kernels are compiled for (register budget).
+#ifndef TBG_MINB_VERIFY
+#define TBG_MINB_VERIFY 4
+#endif
+#ifndef TBG_MINB_SCATTER
+#define TBG_MINB_SCATTER 4
+#endif
+
 constexpr int kThreads = 256;
 constexpr int kTileWords = kThreads * 4;      // 1024 words = 32768 positions
 constexpr int kListCap = 4096;
@@ -35,6 +43,7 @@ __constant__ int c_stub_mod;
 // toggles applied first (a move is a toggle of two bits; a capture removes
 // one; an uncapture adds one), then the normalisation transform.  Sets
 // below kfrom keep the contribution idx0 and the occupancy occ0.
+template <int NS>
 __device__ __forceinline__ uint64_t rank_mod(const DIdx &X, const uint32_t *bin, int k0,
                                             int k1, const bb *set, int ka, bb xa, int kb,
                                             bb xb, int mirror, int flip, int kfrom = 0,
@@ -42,8 +51,8 @@ __device__ __forceinline__ uint64_t rank_mod(const DIdx &X, const uint32_t *bin,
   bb occ = kfrom == 0 ? (bit(k0) | bit(k1)) : occ0;
   uint64_t idx = kfrom == 0 ? 0 : idx0;
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) {
-    if (k >= kfrom && k < X.numsets) {
+  for (int k = 0; k < NS; k++) {
+    if (k >= kfrom) {
       bb b = set[k];
       if (k == ka) b ^= xa;
       if (k == kb) b ^= xb;
@@ -103,127 +112,357 @@ __device__ __forceinline__ bool test_sub(const uint8_t *sub, uint64_t len, uint6
 }
 
 // ------------------------------------------------------ tile compaction
-// Calls f(idx) for every set bit idx < nbits of bits[].  If clr is given,
-// f returns true to clear the bit and the tile is written back in place.
-// With kClear and out != nullptr the surviving bits go to out (every word
-// of the scanned range, out = in & ~cleared) and bits[] is left untouched.
-template <bool kClear, class F>
-__device__ __forceinline__ void scan_tiles(uint32_t *bits, uint64_t nbits, uint32_t *list,
-                                           uint32_t *clr, int *list_n, F &&f,
-                                           uint32_t *out = nullptr) {
-  const uint64_t nwords = (nbits + 31) >> 5;
-  const uint64_t ntiles = (nwords + kTileWords - 1) / kTileWords;
+// Calls f(idx) for every set bit idx < nbits of bits[].  If kClear, f
+// returns true to clear the bit and the tile is written back in place, or,
+// with out != nullptr, the surviving bits of every word of the scanned range
+// go to out (out = in & ~cleared) and bits[] is left untouched.
+// With kContig each thread takes a contiguous run of the tile's list (in
+// index order within each warp's segment) so that consecutive positions of
+// one thread share their leading index digits; otherwise entries go
+// round-robin.  begin(t) runs (block-wide) before the tile's entries,
+// end(t) after them.
+struct NoHook {
+  __device__ void operator()(uint64_t) const {}
+};
+
+// One compaction round: appends the set bits of w[0..3] (this thread's four
+// words of the tile) to list[] while there is room, clearing them from w;
+// returns the number of entries (capped at kListCap).  Block-wide.
+__device__ __forceinline__ int compact_round(uint32_t *w, uint32_t *list, int *list_n) {
   const int lane = threadIdx.x & 31;
-  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const uint64_t w0 = t * kTileWords + threadIdx.x * 4;
-    uint32_t w[4];
-    if (w0 + 4 <= nwords) {
-      uint4 v = *reinterpret_cast<const uint4 *>(bits + w0);
-      w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
-    } else {
+  if (threadIdx.x == 0) *list_n = 0;
+  __syncthreads();
+  int c = __popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]);
+  int incl = c;
 #pragma unroll
-      for (int i = 0; i < 4; i++) w[i] = w0 + i < nwords ? bits[w0 + i] : 0u;
-    }
-    uint32_t raw[4] = {w[0], w[1], w[2], w[3]};
+  for (int d = 1; d < 32; d <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += y;
+  }
+  int base = 0;
+  if (lane == 31) base = atomicAdd(list_n, incl);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  int pos = base + incl - c;
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      uint64_t base = (w0 + i) * 32;
-      if (base + 32 > nbits) w[i] &= base < nbits ? (1u << (nbits - base)) - 1u : 0u;
-    }
-    if (kClear) {
-#pragma unroll
-      for (int i = 0; i < 4; i++) clr[threadIdx.x * 4 + i] = 0;
-    }
-    for (;;) {
-      if (threadIdx.x == 0) *list_n = 0;
-      __syncthreads();
-      int c = __popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]);
-      int incl = c;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d) incl += y;
-      }
-      int base = 0;
-      if (lane == 31) base = atomicAdd(list_n, incl);
-      base = __shfl_sync(0xffffffffu, base, 31);
-      int pos = base + incl - c;
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        while (w[i] && pos < kListCap) {
-          int b = __ffs(w[i]) - 1;
-          w[i] &= w[i] - 1;
-          list[pos++] = (uint32_t)((threadIdx.x * 4 + i) * 32 + b);
-        }
-      }
-      __syncthreads();
-      int n = min(*list_n, kListCap);
-      const uint64_t tbase = t * (uint64_t)kTileWords * 32;
-      for (int e = threadIdx.x; e < n; e += blockDim.x) {
-        uint32_t off = list[e];
-        bool c2 = f(tbase + off);
-        if (kClear && c2) atomicOr(&clr[off >> 5], 1u << (off & 31));
-      }
-      if (!__syncthreads_or((w[0] | w[1] | w[2] | w[3]) != 0)) break;
-    }
-    if (kClear) {
-      __syncthreads();
-      if (out != nullptr) {
-        if (w0 + 4 <= nwords) {
-          uint4 v = make_uint4(raw[0] & ~clr[threadIdx.x * 4], raw[1] & ~clr[threadIdx.x * 4 + 1],
-                               raw[2] & ~clr[threadIdx.x * 4 + 2], raw[3] & ~clr[threadIdx.x * 4 + 3]);
-          *reinterpret_cast<uint4 *>(out + w0) = v;
-        } else {
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-            if (w0 + i < nwords) out[w0 + i] = raw[i] & ~clr[threadIdx.x * 4 + i];
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          uint32_t cm = clr[threadIdx.x * 4 + i];
-          if (cm && w0 + i < nwords) bits[w0 + i] &= ~cm;
-        }
-      }
-      __syncthreads();
+  for (int i = 0; i < 4; i++) {
+    while (w[i] && pos < kListCap) {
+      int b = __ffs(w[i]) - 1;
+      w[i] &= w[i] - 1;
+      list[pos++] = (uint32_t)((threadIdx.x * 4 + i) * 32 + b);
     }
   }
+  __syncthreads();
+  return min(*list_n, kListCap);
+}
+
+// This thread's contiguous share [e0, e1) of n list entries.
+__device__ __forceinline__ void my_share(int n, int &e0, int &e1) {
+  e0 = (int)(((long)n * threadIdx.x) / blockDim.x);
+  e1 = (int)(((long)n * (threadIdx.x + 1)) / blockDim.x);
+}
+
+// The verify's scan of one tile in two passes per compaction round: quick(idx)
+// runs on every candidate and returns 0 (refuted), 1 (survives the quick
+// test); the survivors are compacted into list2 and full(idx) (true:
+// refuted) runs on them only.  Work per thread is then nearly uniform in the
+// first pass, and the divergent full check runs on a dense list.
+template <class Q, class F>
+__device__ __forceinline__ void scan_tile_verify(uint64_t t, uint32_t *bits, uint64_t nbits,
+                                                 uint32_t *list, uint32_t *list2, uint32_t *clr,
+                                                 int *list_n, int *n2, Q &&quick, F &&full,
+                                                 uint32_t *out) {
+  const uint64_t nwords = (nbits + 31) >> 5;
+  const uint64_t w0 = t * kTileWords + threadIdx.x * 4;
+  uint32_t w[4];
+  if (w0 + 4 <= nwords) {
+    uint4 v = *reinterpret_cast<const uint4 *>(bits + w0);
+    w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; i++) w[i] = w0 + i < nwords ? bits[w0 + i] : 0u;
+  }
+  uint32_t raw[4] = {w[0], w[1], w[2], w[3]};
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    uint64_t base = (w0 + i) * 32;
+    if (base + 32 > nbits) w[i] &= base < nbits ? (1u << (nbits - base)) - 1u : 0u;
+    clr[threadIdx.x * 4 + i] = 0;
+  }
+  const uint64_t tbase = t * (uint64_t)kTileWords * 32;
+  for (;;) {
+    if (threadIdx.x == 0) *n2 = 0;
+    const int n = compact_round(w, list, list_n);
+    int e0, e1;
+    my_share(n, e0, e1);
+    for (int e = e0; e < e1; e++) {
+      uint32_t off = list[e];
+      if (quick(tbase + off)) list2[atomicAdd(n2, 1)] = off;
+      else atomicOr(&clr[off >> 5], 1u << (off & 31));
+    }
+    __syncthreads();
+    const int m = *n2;
+    my_share(m, e0, e1);
+    for (int e = e0; e < e1; e++) {
+      uint32_t off = list2[e];
+      if (full(tbase + off)) atomicOr(&clr[off >> 5], 1u << (off & 31));
+    }
+    if (!__syncthreads_or((w[0] | w[1] | w[2] | w[3]) != 0)) break;
+  }
+  __syncthreads();
+  if (out != nullptr) {
+    if (w0 + 4 <= nwords) {
+      uint4 v = make_uint4(raw[0] & ~clr[threadIdx.x * 4], raw[1] & ~clr[threadIdx.x * 4 + 1],
+                           raw[2] & ~clr[threadIdx.x * 4 + 2], raw[3] & ~clr[threadIdx.x * 4 + 3]);
+      *reinterpret_cast<uint4 *>(out + w0) = v;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        if (w0 + i < nwords) out[w0 + i] = raw[i] & ~clr[threadIdx.x * 4 + i];
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      uint32_t cm = clr[threadIdx.x * 4 + i];
+      if (cm && w0 + i < nwords) bits[w0 + i] &= ~cm;
+    }
+  }
+  __syncthreads();
+}
+
+template <bool kClear, bool kContig, class F, class B = NoHook, class E = NoHook>
+__device__ __forceinline__ void scan_tile(uint64_t t, uint32_t *bits, uint64_t nbits,
+                                          uint32_t *list, uint32_t *clr, int *list_n, F &&f,
+                                          uint32_t *out = nullptr, B begin = B(), E end = E()) {
+  const uint64_t nwords = (nbits + 31) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = t * kTileWords + threadIdx.x * 4;
+  uint32_t w[4];
+  if (w0 + 4 <= nwords) {
+    uint4 v = *reinterpret_cast<const uint4 *>(bits + w0);
+    w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; i++) w[i] = w0 + i < nwords ? bits[w0 + i] : 0u;
+  }
+  uint32_t raw[4] = {w[0], w[1], w[2], w[3]};
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    uint64_t base = (w0 + i) * 32;
+    if (base + 32 > nbits) w[i] &= base < nbits ? (1u << (nbits - base)) - 1u : 0u;
+  }
+  if (kClear) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) clr[threadIdx.x * 4 + i] = 0;
+  }
+  begin(t);
+  for (;;) {
+    if (threadIdx.x == 0) *list_n = 0;
+    __syncthreads();
+    int c = __popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]);
+    int incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += y;
+    }
+    int base = 0;
+    if (lane == 31) base = atomicAdd(list_n, incl);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    int pos = base + incl - c;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      while (w[i] && pos < kListCap) {
+        int b = __ffs(w[i]) - 1;
+        w[i] &= w[i] - 1;
+        list[pos++] = (uint32_t)((threadIdx.x * 4 + i) * 32 + b);
+      }
+    }
+    __syncthreads();
+    const int n = min(*list_n, kListCap);
+    const uint64_t tbase = t * (uint64_t)kTileWords * 32;
+    int e0, e1, es;
+    if (kContig) {
+      e0 = (int)(((long)n * threadIdx.x) / blockDim.x);
+      e1 = (int)(((long)n * (threadIdx.x + 1)) / blockDim.x);
+      es = 1;
+    } else {
+      e0 = threadIdx.x;
+      e1 = n;
+      es = blockDim.x;
+    }
+    for (int e = e0; e < e1; e += es) {
+      uint32_t off = list[e];
+      bool c2 = f(tbase + off);
+      if (kClear && c2) atomicOr(&clr[off >> 5], 1u << (off & 31));
+    }
+    if (!__syncthreads_or((w[0] | w[1] | w[2] | w[3]) != 0)) break;
+  }
+  end(t);
+  if (kClear) {
+    __syncthreads();
+    if (out != nullptr) {
+      if (w0 + 4 <= nwords) {
+        uint4 v = make_uint4(raw[0] & ~clr[threadIdx.x * 4], raw[1] & ~clr[threadIdx.x * 4 + 1],
+                             raw[2] & ~clr[threadIdx.x * 4 + 2], raw[3] & ~clr[threadIdx.x * 4 + 3]);
+        *reinterpret_cast<uint4 *>(out + w0) = v;
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          if (w0 + i < nwords) out[w0 + i] = raw[i] & ~clr[threadIdx.x * 4 + i];
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        uint32_t cm = clr[threadIdx.x * 4 + i];
+        if (cm && w0 + i < nwords) bits[w0 + i] &= ~cm;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ uint64_t tiles_of(uint64_t nbits) {
+  return (((nbits + 31) >> 5) + kTileWords - 1) / kTileWords;
+}
+
+// ------------------------------------------------------- incremental deindex
+// Positions of one row (all digits but the last set's equal) share the
+// sets 0..L-1 (L = numsets - 1); a thread walking increasing indices keeps
+// them and re-unranks only the last set while the row does not change.
+struct RowCache {
+  uint64_t row = ~0ull;
+  uint64_t row_base = 0;   // index of the row's first position
+  bb occ_head = 0;         // kings + sets 0..L-1
+};
+
+template <int NS>
+__device__ __forceinline__ bb unrank_cached(const DIdx &X, const uint32_t *bin, uint64_t idx,
+                                           int k0, int k1, bb *set, RowCache &rc) {
+  constexpr int L = NS - 1;
+  uint64_t row = 0, F = X.size;
+  if (L > 0) {
+    F = X.factor[L > 0 ? L - 1 : 0];
+    row = idx < (1ull << 32) ? fast_div32((uint32_t)idx, X.fdiv[L > 0 ? L - 1 : 0]) : idx / F;
+  }
+  if (row != rc.row) {
+    bb occ = unrank_sets<NS>(X, bin, idx, k0, k1, set);
+    bb last = 0;
+#pragma unroll
+    for (int k = 0; k < NS; k++)
+      if (k == L) last = set[k];
+    rc.row = row;
+    rc.row_base = row * F;
+    rc.occ_head = occ & ~last;
+    return occ;
+  }
+  // same row: only the last set changes
+  uint32_t d = (uint32_t)(idx - rc.row_base);
+  bb freeb = ~rc.occ_head, sb = 0;
+  int m = X.mult[L];
+  for (int i = m - 1; i > 0; i--) {
+    const uint32_t *rowb = bin + (i + 1) * 64;
+    int lo = i, hi = 63;
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (rowb[mid] <= d) lo = mid;
+      else hi = mid;
+    }
+    d -= rowb[lo];
+    sb |= bit(nth_set(freeb, lo));
+  }
+  if (m > 0) sb |= bit(nth_set(freeb, (int)d));
+#pragma unroll
+  for (int k = 0; k < NS; k++)
+    if (k == L) set[k] = sb;
+  return rc.occ_head | sb;
 }
 
 // ----------------------------------------------------------- W step
 // mark_king_unmoves (tb8gen.c:246-262) for a position with an optional
 // uncaptured piece (set kb, square xb) on the king's old square.
-__device__ __forceinline__ void mark_king_unmoves(const SliceJob &J, const DMat &M,
-                                                  const uint32_t *bin, const bb *set, bb occ,
-                                                  int kb, bb xb, DevStatus *st) {
+template <int NS>
+__device__ __forceinline__ void mark_king_unmoves(const SliceJob &J, const KingDest *kd,
+                                                  const DMat &M, const uint32_t *bin,
+                                                  const bb *set, bb occ, int kb, bb xb,
+                                                  DevStatus *st) {
   int opp = J.stm ? J.k0 : J.k1;
   bb dest = ~(occ | king_attacks(opp));
   for (int d = 0; d < J.nk; d++) {
-    const KingDest &D = J.kd[d];
+    const KingDest &D = kd[d];
     if (!(dest & bit(D.to))) continue;
-    uint64_t i = rank_mod(M.ii, bin, D.k0, D.k1, set, -1, 0, kb, xb, D.mirror, D.flip);
+    uint64_t i = rank_mod<NS>(M.ii, bin, D.k0, D.k1, set, -1, 0, kb, xb, D.mirror, D.flip);
     mark(D.bits, i, M.ii.size, st);
     if (D.dbl) {
       // mirror_diagonal (tb8gen.c:240-244) of the normalised position: the
       // kings are on the diagonal, so the transpose acts on the sets only.
       int m2 = D.mirror;
-      uint64_t i2 = rank_mod(M.ii, bin, D.k0, D.k1, set, -1, 0, kb, xb, m2, D.flip ^ 1);
+      uint64_t i2 = rank_mod<NS>(M.ii, bin, D.k0, D.k1, set, -1, 0, kb, xb, m2, D.flip ^ 1);
       mark(D.bits, i2, M.ii.size, st);
     }
   }
 }
 
+// The king destinations, copied from the kernel parameters into shared
+// memory once per block (indexed at run time below).
+__device__ __forceinline__ void load_dests(const SliceJob &J, KingDest *kd) {
+#pragma unroll
+  for (int d = 0; d < 8; d++)
+    if (threadIdx.x == d) kd[d] = J.kd[d];
+}
+
+// Marks into the slice's own bitmap that land near the tile being scanned
+// go to a shared-memory window first and reach HBM as one atomicOr per
+// touched word when the tile ends: moves of the last (fastest-varying) set
+// stay in their row, so most marks of such moves are local.
+constexpr int kWinWords = 3072;                     // 98,304 positions, 12 KB
+constexpr int64_t kWinLead = 32768;                 // window starts one tile early
+
+struct Window {
+  uint32_t *w;      // nullptr: no window
+  int64_t base;     // first position of the window (a multiple of 32)
+};
+
+__device__ __forceinline__ void mark_self(const SliceJob &J, const DMat &M, const Window &W,
+                                          uint64_t i, DevStatus *st) {
+  if (W.w != nullptr) {
+    int64_t r = (int64_t)i - W.base;
+    if ((uint64_t)r < (uint64_t)kWinWords * 32 && i < M.ii.size) {
+      atomicOr(&W.w[r >> 5], 1u << (r & 31));
+      return;
+    }
+  }
+  mark(J.self, i, M.ii.size, st);
+}
+
+__device__ __forceinline__ void window_clear(uint32_t *win) {
+  for (int i = threadIdx.x; i < kWinWords; i += blockDim.x) win[i] = 0;
+}
+
+__device__ __forceinline__ void window_flush(uint32_t *win, int64_t base, uint32_t *bits,
+                                             uint64_t nwords) {
+  __syncthreads();
+  const int64_t w0 = base / 32;
+  for (int i = threadIdx.x; i < kWinWords; i += blockDim.x) {
+    uint32_t v = win[i];
+    int64_t gw = w0 + i;
+    if (v && gw >= 0 && (uint64_t)gw < nwords) atomicOr(bits + gw, v);
+  }
+  __syncthreads();
+}
+
 // mark_unmoves (tb8gen.c:264-276) for every non-king piece of the side to
 // move, optionally with an uncaptured piece (set kb, square taken from the
 // moving piece's origin).
+template <int NS>
 __device__ __forceinline__ void mark_piece_unmoves(const SliceJob &J, const DMat &M,
                                                    const uint32_t *bin, const bb *set,
-                                                   bb occ, int kb, DevStatus *st) {
+                                                   bb occ, int kb, const Window &W,
+                                                   DevStatus *st) {
   bb occk = bit(J.k0) | bit(J.k1);
   uint64_t idxk = 0;
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) {
-    if (k < M.ii.numsets && M.set_color[k] == J.stm) {
+  for (int k = 0; k < NS; k++) {
+    if (M.set_color[k] == J.stm) {
       bb pcs = set[k];
       while (pcs) {
         int x = pop_lsb(pcs);
@@ -232,16 +471,16 @@ __device__ __forceinline__ void mark_piece_unmoves(const SliceJob &J, const DMat
           int to = pop_lsb(mv);
           uint64_t i;
           if (kb < 0)
-            i = rank_mod(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0, k,
+            i = rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0, k,
                          occk, idxk);
           else
-            i = rank_mod(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), kb, bit(x), 0, 0);
-          mark(J.self, i, M.ii.size, st);
+            i = rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), kb, bit(x), 0, 0);
+          mark_self(J, M, W, i, st);
         }
       }
     }
     // Sets below the next moving set keep their rank contribution.
-    if (k < M.ii.numsets) {
+    {
       bb b = set[k];
       bb occ2 = occk | b;
       uint32_t s = 0;
@@ -257,135 +496,279 @@ __device__ __forceinline__ void mark_piece_unmoves(const SliceJob &J, const DMat
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_predecessors(SliceJob J, DevStatus *st) {
-  __shared__ uint32_t bin[7 * 64];
-  __shared__ uint32_t list[kListCap];
-  __shared__ int list_n;
-  load_binomials(bin);
-  __syncthreads();
+// Shared memory of the sparse kernels (one tile at a time).
+struct SparseSmem {
+  uint32_t bin[7 * 64];
+  KingDest kd[8];
+  uint32_t list[kListCap];
+  union {
+    uint32_t win[kWinWords];   // scatter: the staging window
+    struct {
+      uint32_t clr[kTileWords];   // verify: cleared candidates of the tile
+      uint32_t list2[kListCap];   // verify: survivors of the quick test
+    };
+  };
+  int list_n;
+  int n2;
+};
+
+// One tile of predecessors_worker (tb8gen.c:484-516).
+template <int NS>
+__device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem &S, uint64_t t,
+                                                  DevStatus *st) {
   const DMat &M = c_mats[J.mat];
-  scan_tiles<false>(const_cast<uint32_t *>(J.src), J.nbits, list, nullptr, &list_n,
-                    [&](uint64_t idx) {
-                      bb set[TBG_MAX_SETS];
-                      bb occ = unrank_sets(M.ii, bin, idx, J.k0, J.k1, set);
-                      mark_king_unmoves(J, M, bin, set, occ, -1, 0, st);
-                      mark_piece_unmoves(J, M, bin, set, occ, -1, st);
-                      return false;
-                    });
+  const uint64_t self_words = (M.ii.size + 31) >> 5;
+  Window W{S.win, 0};
+  bb set[NS];
+  RowCache rc;
+  scan_tile<false, true>(
+      t, const_cast<uint32_t *>(J.src), J.nbits, S.list, nullptr, &S.list_n,
+      [&](uint64_t idx) {
+        bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
+        mark_king_unmoves<NS>(J, S.kd, M, S.bin, set, occ, -1, 0, st);
+        mark_piece_unmoves<NS>(J, M, S.bin, set, occ, -1, W, st);
+        return false;
+      },
+      nullptr,
+      [&](uint64_t tt) {
+        window_clear(S.win);
+        W.base = (int64_t)(tt * (uint64_t)kTileWords * 32) - kWinLead;
+      },
+      [&](uint64_t) { window_flush(S.win, W.base, J.self, self_words); });
+}
+
+template <int NS>
+__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors(SliceJob J, DevStatus *st) {
+  __shared__ SparseSmem S;
+  load_dests(J, S.kd);
+  load_binomials(S.bin);
+  __syncthreads();
+  const uint64_t nt = tiles_of(J.nbits);
+  for (uint64_t t = blockIdx.x; t < nt; t += gridDim.x) tile_predecessors<NS>(J, S, t, st);
 }
 
 // predecessors_sub_worker (tb8gen.c:346-394): the source is the sub bitmap
 // of captured set J.set (colour stm^1); each position is uncaptured by the
 // king and by every non-king piece of stm.
-__global__ void __launch_bounds__(kThreads) k_predecessors_sub(SliceJob J, DevStatus *st) {
-  __shared__ uint32_t bin[7 * 64];
-  __shared__ uint32_t list[kListCap];
-  __shared__ int list_n;
-  load_binomials(bin);
-  __syncthreads();
+template <int NS>
+__device__ __forceinline__ void tile_predecessors_sub(const SliceJob &J, SparseSmem &S,
+                                                      uint64_t t, DevStatus *st) {
   const DMat &M = c_mats[J.mat];
   const int kc = J.set;
   const DIdx &X = M.capt[kc];
-  scan_tiles<false>(const_cast<uint32_t *>(J.src), J.nbits, list, nullptr, &list_n,
-                    [&](uint64_t idx) {
-                      bb set[TBG_MAX_SETS];
-                      bb occ = unrank_sets(X, bin, idx, J.k0, J.k1, set);
-                      int me = J.stm ? J.k1 : J.k0;
-                      if (J.legality &&
-                          attacked_by(M, set, J.k0, J.k1, occ, me, J.stm ^ 1))
-                        return false;
-                      mark_king_unmoves(J, M, bin, set, occ, kc, bit(me), st);
-                      mark_piece_unmoves(J, M, bin, set, occ, kc, st);
-                      return false;
-                    });
+  const Window W{nullptr, 0};
+  bb set[NS];
+  RowCache rc;
+  scan_tile<false, true>(t, const_cast<uint32_t *>(J.src), J.nbits, S.list, nullptr, &S.list_n,
+                         [&](uint64_t idx) {
+                           bb occ = unrank_cached<NS>(X, S.bin, idx, J.k0, J.k1, set, rc);
+                           int me = J.stm ? J.k1 : J.k0;
+                           if (J.legality &&
+                               attacked_by<NS>(M, set, J.k0, J.k1, occ, me, J.stm ^ 1))
+                             return false;
+                           mark_king_unmoves<NS>(J, S.kd, M, S.bin, set, occ, kc, bit(me), st);
+                           mark_piece_unmoves<NS>(J, M, S.bin, set, occ, kc, W, st);
+                           return false;
+                         });
+}
+
+template <int NS>
+__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors_sub(SliceJob J, DevStatus *st) {
+  __shared__ SparseSmem S;
+  load_dests(J, S.kd);
+  load_binomials(S.bin);
+  __syncthreads();
+  const uint64_t nt = tiles_of(J.nbits);
+  for (uint64_t t = blockIdx.x; t < nt; t += gridDim.x) tile_predecessors_sub<NS>(J, S, t, st);
 }
 
 // ----------------------------------------------------------- L step
 // check_successors_worker (tb8gen.c:607-650) with check_moves (571-605) and
 // check_king_moves (537-569).  True iff the candidate is to be cleared.
-__device__ __forceinline__ bool refute(const SliceJob &J, const DMat &M, const uint32_t *bin,
-                                       uint64_t idx, DevStatus *st) {
-  bb set[TBG_MAX_SETS];
-  bb occ = unrank_sets(M.ii, bin, idx, J.k0, J.k1, set);
+//
+// A candidate survives iff it is legal and every successor is won for the
+// opponent: a conjunction, so the tests may run in any order as long as the
+// king captures, whose capture index the reference computes in its own way
+// (see below), are reached exactly when the reference reaches them -- after
+// legality and every non-king piece passed.  The quiet moves of the side's
+// sets run first, the last set first: they are the cheapest (only the sets
+// from the moving one on are re-ranked) and, at the densities of a ply, the
+// most likely to refute.
+template <int NS>
+__device__ __forceinline__ bool refute(const SliceJob &J, const KingDest *kd, const DMat &M,
+                                       const uint32_t *bin, const bb *set, bb occ,
+                                       const RowCache &rc, DevStatus *st) {
   const int stm = J.stm;
-  const int me = stm ? J.k1 : J.k0, opp = stm ? J.k0 : J.k1;
-  if (attacked_by(M, set, J.k0, J.k1, occ, opp, stm)) return true;
+  const int opp = stm ? J.k0 : J.k1;
+  // rank prefixes: occupancy and index contribution of the sets below k.
+  // Set 0's is the kings alone; the last set's comes from the row cache;
+  // the ones between are computed.
+  bb pre_occ[NS];
+  uint64_t pre_idx[NS];
+  pre_occ[0] = bit(J.k0) | bit(J.k1);
+  pre_idx[0] = 0;
+  if (NS > 1) {
+    pre_occ[NS - 1] = rc.occ_head;
+    pre_idx[NS - 1] = rc.row_base;
+  }
+  if (NS > 2) {
+    bb o = pre_occ[0];
+    uint64_t ix = 0;
+#pragma unroll
+    for (int k = 0; k < NS - 2; k++) {
+      bb b = set[k];
+      bb o2 = o | b;
+      uint32_t sm = 0;
+      int j = 1;
+      while (b) {
+        int x = pop_lsb(b);
+        sm += bin[j * 64 + x - __popcll(o & (bit(x) - 1))];
+        j++;
+      }
+      ix += (uint64_t)sm * M.ii.factor[k];
+      o = o2;
+      pre_occ[k + 1] = o;
+      pre_idx[k + 1] = ix;
+    }
+  }
   bb own = 0;
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++)
-    if (k < M.ii.numsets && M.set_color[k] == stm) own |= set[k];
-  // Non-king pieces: captures must lead into sub/win, quiet moves into wins.
+  for (int k = 0; k < NS; k++)
+    if (M.set_color[k] == stm) own |= set[k];
+  // 1. quiet moves of the non-king pieces into "wins"
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) {
-    if (k < M.ii.numsets && M.set_color[k] == stm) {
+  for (int k = NS - 1; k >= 0; k--) {
+    if (M.set_color[k] == stm) {
       bb pcs = set[k];
       while (pcs) {
         int x = pop_lsb(pcs);
-        bb att = piece_attacks(M.set_type[k], x, occ);
-        bb caps = att & occ & ~own & ~bit(opp);
-        while (caps) {
-          int to = pop_lsb(caps);
-#pragma unroll
-          for (int l = 0; l < TBG_MAX_SETS; l++) {
-            if (l < M.ii.numsets && (set[l] & bit(to))) {
-              uint64_t i = rank_mod(M.capt[l], bin, J.k0, J.k1, set, k, bit(x) | bit(to), l,
-                                    bit(to), 0, 0);
-              if (!test_sub(J.self_sub, J.self_sub_len, M.sub_offset[l], i, st)) return true;
-            }
-          }
-        }
-        bb quiet = att & ~occ;
+        bb quiet = piece_attacks(M.set_type[k], x, occ) & ~occ;
         while (quiet) {
           int to = pop_lsb(quiet);
-          uint64_t i = rank_mod(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0);
+          uint64_t i = rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0, k,
+                                pre_occ[k], pre_idx[k]);
           if (!test(J.self, i, M.ii.size, st)) return true;
         }
       }
     }
   }
-  // King: captures leave the captured piece in its slot and drop the set's
+  // 2. legality: the side to move must not attack the other king
+  if (attacked_by<NS>(M, set, J.k0, J.k1, occ, opp, stm)) return true;
+  // 3. captures by the non-king pieces into sub/win
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    if (M.set_color[k] == stm) {
+      bb pcs = set[k];
+      while (pcs) {
+        int x = pop_lsb(pcs);
+        bb caps = piece_attacks(M.set_type[k], x, occ) & occ & ~own & ~bit(opp);
+        while (caps) {
+          int to = pop_lsb(caps);
+#pragma unroll
+          for (int l = 0; l < NS; l++) {
+            if (set[l] & bit(to)) {
+              uint64_t i = rank_mod<NS>(M.capt[l], bin, J.k0, J.k1, set, k, bit(x) | bit(to), l,
+                                    bit(to), 0, 0);
+              if (!test_sub(J.self_sub, J.self_sub_len, M.sub_offset[l], i, st)) return true;
+            }
+          }
+        }
+      }
+    }
+  }
+  // 4. King captures leave the captured piece in its slot and drop the set's
   // last slot (its highest square) from the capture index, as the reference
-  // computes it (tb8gen.c:543-555); quiet moves go to neighbouring slices.
+  // computes it (tb8gen.c:543-555).
   for (int d = 0; d < J.nk; d++) {
-    const KingDest &D = J.kd[d];
+    const KingDest &D = kd[d];
     if (!(occ & bit(D.to))) continue;
     if (own & bit(D.to)) continue;
 #pragma unroll
-    for (int l = 0; l < TBG_MAX_SETS; l++) {
-      if (l < M.ii.numsets && (set[l] & bit(D.to))) {
-        uint64_t i = rank_mod(M.capt[l], bin, D.k0, D.k1, set, -1, 0, l,
+    for (int l = 0; l < NS; l++) {
+      if (set[l] & bit(D.to)) {
+        uint64_t i = rank_mod<NS>(M.capt[l], bin, D.k0, D.k1, set, -1, 0, l,
                               bit(msb64(set[l])), D.mirror, D.flip);
         if (!test_sub(D.sub, D.sub_len, M.sub_offset[l], i, st)) return true;
       }
     }
   }
+  // 5. quiet king moves into the neighbouring slices' "wins"
   for (int d = 0; d < J.nk; d++) {
-    const KingDest &D = J.kd[d];
+    const KingDest &D = kd[d];
     if (occ & bit(D.to)) continue;
-    uint64_t i = rank_mod(M.ii, bin, D.k0, D.k1, set, -1, 0, -1, 0, D.mirror, D.flip);
+    uint64_t i = rank_mod<NS>(M.ii, bin, D.k0, D.k1, set, -1, 0, -1, 0, D.mirror, D.flip);
     if (!test(D.bits, i, M.ii.size, st)) return true;
   }
-  (void)me;
   return false;
 }
 
+// The quick test of the verify: the first quiet move of the side's pieces,
+// last set first, must lead into "wins".  Returns false when that refutes the
+// candidate, true when the candidate needs the full check.
+template <int NS>
+__device__ __forceinline__ bool survives_quick(const SliceJob &J, const DMat &M,
+                                               const uint32_t *bin, const bb *set, bb occ,
+                                               const RowCache &rc, DevStatus *st) {
+#pragma unroll
+  for (int k = NS - 1; k >= 0; k--) {
+    if (M.set_color[k] == J.stm) {
+      bb pcs = set[k];
+      while (pcs) {
+        int x = pop_lsb(pcs);
+        bb quiet = piece_attacks(M.set_type[k], x, occ) & ~occ;
+        if (quiet) {
+          int to = ctz64(quiet);
+          bb po = k == 0 ? (bit(J.k0) | bit(J.k1)) : (k == NS - 1 ? rc.occ_head : 0);
+          uint64_t pi = k == NS - 1 ? rc.row_base : 0;
+          uint64_t i = (k == 0 || k == NS - 1)
+                           ? rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0,
+                                          0, 0, k, po, pi)
+                           : rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0,
+                                          0, 0);
+          return test(J.self, i, M.ii.size, st);
+        }
+      }
+    }
+  }
+  return true;
+}
+
 // Candidates are read from J.cand; survivors are written back in place, or
-// to `out` (every word up to out_words; words past the scanned range copied).
-__global__ void __launch_bounds__(kThreads) k_check_successors(SliceJob J, DevStatus *st,
-                                                               uint32_t *out, uint64_t out_words) {
-  __shared__ uint32_t bin[7 * 64];
-  __shared__ uint32_t list[kListCap];
-  __shared__ uint32_t clr[kTileWords];
-  __shared__ int list_n;
-  load_binomials(bin);
-  __syncthreads();
+// to `out` (every word up to out_words; words past the scanned range copied
+// by the block that owns tile 0).
+template <int NS>
+__device__ __forceinline__ void tile_check(const SliceJob &J, SparseSmem &S, uint64_t t,
+                                           DevStatus *st, uint32_t *out, uint64_t out_words) {
   const DMat &M = c_mats[J.mat];
-  scan_tiles<true>(J.cand, J.nbits, list, clr, &list_n,
-                   [&](uint64_t idx) { return refute(J, M, bin, idx, st); }, out);
-  if (out != nullptr && blockIdx.x == 0) {
+  bb set[NS];
+  RowCache rc;
+  scan_tile_verify(
+      t, J.cand, J.nbits, S.list, S.list2, S.clr, &S.list_n, &S.n2,
+      [&](uint64_t idx) {
+        bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
+        return survives_quick<NS>(J, M, S.bin, set, occ, rc, st);
+      },
+      [&](uint64_t idx) {
+        bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
+        return refute<NS>(J, S.kd, M, S.bin, set, occ, rc, st);
+      },
+      out);
+  if (out != nullptr && t == 0) {
     for (uint64_t w = ((J.nbits + 31) >> 5) + threadIdx.x; w < out_words; w += blockDim.x)
       out[w] = J.cand[w];
   }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(kThreads, TBG_MINB_VERIFY) k_check_successors(SliceJob J, DevStatus *st,
+                                                                  uint32_t *out,
+                                                                  uint64_t out_words) {
+  __shared__ SparseSmem S;
+  load_dests(J, S.kd);
+  load_binomials(S.bin);
+  __syncthreads();
+  const uint64_t nt = tiles_of(J.nbits);
+  for (uint64_t t = blockIdx.x; t < nt; t += gridDim.x) tile_check<NS>(J, S, t, st, out, out_words);
 }
 
 // ------------------------------------------------ dense per-position kernels
@@ -399,12 +782,13 @@ __device__ __forceinline__ uint64_t piece_key(int type, int sq) {
   return mix64(((uint64_t)((type << 6) | sq)) * kGamma + kGamma);
 }
 
+template <int NS>
 __device__ __forceinline__ int stub_wdl(const DMat &M, const bb *set, int k0, int k1, int stm) {
   uint64_t key = stm ? kStmKey : 0;
   key ^= piece_key(M.king_type[0], k0) ^ piece_key(M.king_type[1], k1);
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) {
-    if (k < M.ii.numsets) {
+  for (int k = 0; k < NS; k++) {
+    {
       bb b = set[k];
       int t = M.set_type[k] | (M.set_color[k] << 3);
       while (b) key ^= piece_key(t, pop_lsb(b));
@@ -431,6 +815,7 @@ __device__ __forceinline__ void store_partial(uint32_t *p, uint64_t w, uint64_t 
 
 // calc_sub_worker (tb8gen.c:280-314) for captured set J.set of colour stm:
 // cls[0..4] = loss, bloss, draw, cwin, win; illegal positions -> cwin+win.
+template <int NS>
 __global__ void __launch_bounds__(kThreads) k_calc_sub(SliceJob J, uint32_t *c0, uint32_t *c1,
                                                        uint32_t *c2, uint32_t *c3, uint32_t *c4) {
   __shared__ uint32_t bin[7 * 64];
@@ -446,14 +831,14 @@ __global__ void __launch_bounds__(kThreads) k_calc_sub(SliceJob J, uint32_t *c0,
     for (int b = 0; b < 32; b++) {
       uint64_t idx = w * 32 + b;
       if (idx >= n) break;
-      bb set[TBG_MAX_SETS];
-      bb occ = unrank_sets(X, bin, idx, J.k0, J.k1, set);
+      bb set[NS];
+      bb occ = unrank_sets<NS>(X, bin, idx, J.k0, J.k1, set);
       uint32_t m = 1u << b;
-      if (attacked_by(M, set, J.k0, J.k1, occ, opp, stm)) {
+      if (attacked_by<NS>(M, set, J.k0, J.k1, occ, opp, stm)) {
         o[3] |= m;
         o[4] |= m;
       } else {
-        int v = stub_wdl(M, set, J.k0, J.k1, stm);
+        int v = stub_wdl<NS>(M, set, J.k0, J.k1, stm);
         o[v + 2] |= m;
         if (v == 2) o[3] |= m;
       }
@@ -470,6 +855,7 @@ __global__ void __launch_bounds__(kThreads) k_calc_sub(SliceJob J, uint32_t *c0,
 // illegal for colour c to move iff a piece of colour c attacks the other
 // king.  Every word of both outputs is written (padding words zero), as
 // after the kslice_clear_addr of tb8gen.c:738-739.
+template <int NS>
 __global__ void __launch_bounds__(kThreads) k_calc_illegal(SliceJob J, uint32_t *ill_w,
                                                            uint32_t *ill_b, uint64_t nwords) {
   __shared__ uint32_t bin[7 * 64];
@@ -483,10 +869,10 @@ __global__ void __launch_bounds__(kThreads) k_calc_illegal(SliceJob J, uint32_t 
     for (int b = 0; b < 32; b++) {
       uint64_t idx = w * 32 + b;
       if (idx >= n) break;
-      bb set[TBG_MAX_SETS];
-      bb occ = unrank_sets(M.ii, bin, idx, J.k0, J.k1, set);
-      if (attacked_by(M, set, J.k0, J.k1, occ, J.k1, 0)) ow |= 1u << b;
-      if (attacked_by(M, set, J.k0, J.k1, occ, J.k0, 1)) ob |= 1u << b;
+      bb set[NS];
+      bb occ = unrank_sets<NS>(M.ii, bin, idx, J.k0, J.k1, set);
+      if (attacked_by<NS>(M, set, J.k0, J.k1, occ, J.k1, 0)) ow |= 1u << b;
+      if (attacked_by<NS>(M, set, J.k0, J.k1, occ, J.k0, 1)) ob |= 1u << b;
     }
     ill_w[w] = ow;
     ill_b[w] = ob;
@@ -494,16 +880,17 @@ __global__ void __launch_bounds__(kThreads) k_calc_illegal(SliceJob J, uint32_t 
 }
 
 // has_legal_moves || has_legal_caps (movegen.c:75-111) for side stm.
+template <int NS>
 __device__ __forceinline__ bool has_legal(const DMat &M, const bb *set0, int k0, int k1, bb occ,
                                           int stm) {
-  bb set[TBG_MAX_SETS];
+  bb set[NS];
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) set[k] = set0[k];
+  for (int k = 0; k < NS; k++) set[k] = set0[k];
   const int me = stm ? k1 : k0;
   bb own = bit(me), theirs = bit(stm ? k0 : k1);
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++)
-    if (k < M.ii.numsets) {
+  for (int k = 0; k < NS; k++)
+    {
       if (M.set_color[k] == stm) own |= set[k];
       else theirs |= set[k];
     }
@@ -513,16 +900,16 @@ __device__ __forceinline__ bool has_legal(const DMat &M, const bb *set0, int k0,
     int to = pop_lsb(kb);
     bb tb = bit(to);
     int nk0 = stm ? k0 : to, nk1 = stm ? to : k1;
-    bb sv[TBG_MAX_SETS];
+    bb sv[NS];
 #pragma unroll
-    for (int k = 0; k < TBG_MAX_SETS; k++) sv[k] = set[k] & ~tb;
+    for (int k = 0; k < NS; k++) sv[k] = set[k] & ~tb;
     bb occ2 = (occ & ~bit(me)) | tb;
-    if (!attacked_by(M, sv, nk0, nk1, occ2, to, stm ^ 1)) return true;
+    if (!attacked_by<NS>(M, sv, nk0, nk1, occ2, to, stm ^ 1)) return true;
   }
   // Other pieces.
 #pragma unroll
-  for (int k = 0; k < TBG_MAX_SETS; k++) {
-    if (k < M.ii.numsets && M.set_color[k] == stm) {
+  for (int k = 0; k < NS; k++) {
+    if (M.set_color[k] == stm) {
       bb pcs = set[k];
       while (pcs) {
         int x = pop_lsb(pcs);
@@ -530,12 +917,12 @@ __device__ __forceinline__ bool has_legal(const DMat &M, const bb *set0, int k0,
         while (mv) {
           int to = pop_lsb(mv);
           bb tb = bit(to);
-          bb sv[TBG_MAX_SETS];
+          bb sv[NS];
 #pragma unroll
-          for (int q = 0; q < TBG_MAX_SETS; q++) sv[q] = set[q] & ~tb;
+          for (int q = 0; q < NS; q++) sv[q] = set[q] & ~tb;
           sv[k] = (set[k] ^ bit(x)) | tb;
           bb occ2 = (occ & ~bit(x)) | tb;
-          if (!attacked_by(M, sv, k0, k1, occ2, me, stm ^ 1)) return true;
+          if (!attacked_by<NS>(M, sv, k0, k1, occ2, me, stm ^ 1)) return true;
         }
       }
     }
@@ -546,6 +933,7 @@ __device__ __forceinline__ bool has_legal(const DMat &M, const bb *set0, int k0,
 
 // calc_mate_worker (tb8gen.c:686-727): positions legal for exactly one side
 // to move, where that side has no legal move or capture.
+template <int NS>
 __global__ void __launch_bounds__(kThreads) k_calc_mate(SliceJob J, const uint32_t *ill_w,
                                                         const uint32_t *ill_b, uint32_t *mate_w,
                                                         uint32_t *mate_b, uint64_t nwords) {
@@ -563,10 +951,10 @@ __global__ void __launch_bounds__(kThreads) k_calc_mate(SliceJob J, const uint32
       cand &= cand - 1;
       uint64_t idx = w * 32 + b;
       if (idx >= n) break;
-      bb set[TBG_MAX_SETS];
-      bb occ = unrank_sets(M.ii, bin, idx, J.k0, J.k1, set);
+      bb set[NS];
+      bb occ = unrank_sets<NS>(M.ii, bin, idx, J.k0, J.k1, set);
       int stm = (ib >> b) & 1 ? 0 : 1;
-      if (!has_legal(M, set, J.k0, J.k1, occ, stm)) {
+      if (!has_legal<NS>(M, set, J.k0, J.k1, occ, stm)) {
         if (stm == 0) ow |= 1u << b;
         else ob |= 1u << b;
       }

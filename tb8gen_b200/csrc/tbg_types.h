@@ -1,6 +1,8 @@
 // Types shared by the host side of the library and its kernels.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 #define TBG_MAX_SETS 6
@@ -71,6 +73,28 @@ struct DevStatus {
   unsigned int err;
   unsigned int where;
   unsigned long long info;
+};
+
+enum OpKind : int { OP_SCATTER = 1, OP_SCATTER_SUB = 2, OP_VERIFY = 3, OP_EPILOGUE = 4, OP_CLEAR = 5 };
+
+constexpr uint64_t kChunk16 = 1u << 16;   // streaming tile: 65,536 x 16 B = 1 MiB
+
+struct alignas(16) Op {
+  int kind;
+  int ns;                  // piece sets of the material (sparse kernels)
+  uint32_t ntiles;
+  int npred, pred_off;
+  int cnt_slot;            // epilogue count slot of a recorded batch (-1: none)
+  uint64_t first;          // index of the op's first work item
+  SliceJob J;              // sparse kernels
+  uint32_t *out;           // verify: out-of-place output (or null)
+  uint64_t out_words;
+  uint4 *T;                // epilogue / clear target
+  const uint4 *win;        // epilogue: wins in
+  uint4 *wout;             // epilogue: wins out
+  uint64_t n16;            // vectors of T
+  uint64_t nbits;          // epilogue: positions counted
+  unsigned long long *cnt; // epilogue: count slot (or null)
 };
 
 }  // namespace tbg

@@ -260,3 +260,17 @@ class SlicePly:
         tbg.bind(0, self.T)
         tbg.bind(1, self.X)
         return tbg.count(0), tbg.count(1)
+
+
+def record_step(jobs):
+    """Records one step of every job (phase by phase: all W scatters, all
+    epilogues, all L scatters, all verifies) as a batch; returns
+    (recorded calls, work items).  tbg.batch_run(0 | 1) then runs it."""
+    tbg.batch_begin()
+    try:
+        for ph in SlicePly.PHASES:
+            for j in jobs:
+                getattr(j, ph)()
+    finally:
+        n = tbg.batch_end()
+    return n

@@ -1,0 +1,40 @@
+"""The C ABI library: it loads without a GPU, exports every function that
+include/*.h declares, and answers argument errors before touching CUDA."""
+import ctypes as C
+import glob
+import os
+import re
+
+import tb8gen_b200 as tbg
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"^\s*(?:int|const char \*|uint64_t)\s+\**(tbg_\w+)\s*\(", text, re.M))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "tbg_predecessors" in names and "tbg_check_successors" in names
+    assert len(names) >= 20
+
+
+def test_library_exports_every_declared_function():
+    L = tbg.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_argument_errors_without_gpu():
+    L = tbg.lib()
+    assert L.tbg_material_select(99) == -1        # TBG_ERR_ARG
+    assert L.tbg_material_from_name(None) == -1
+    n = C.c_uint64()
+    assert L.tbg_launches(C.byref(n)) == 0
+    assert b"material" in L.tbg_last_error() or L.tbg_last_error() is not None

@@ -1,0 +1,80 @@
+"""The batched ply (tbg_batch_*): a recorded step of several slice-ply jobs
+of two materials gives the same bitmaps through one launch per call
+(mode 0) and through the persistent kernel (mode 1, several grid sizes),
+and each job's W, L and wins equal the reference's CPU workers on the same
+inputs."""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from oracle.plyjob_cpu import CpuSlicePly
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import tb8gen_b200 as tbg
+    from tb8gen_b200.plyjob import MaterialPool, SlicePly, record_step
+
+    tbg.init()
+    tbg.set_stub(1)
+    spec = [("KRRvKR", 96, 0.02), ("KQRvKRR", 300, 0.01), ("KRRvKR", 452, 0.05),
+            ("KQRvKRR", 5, 0.03), ("KRRvKR", 441, 0.01)]
+    pools, jobs = {}, []
+    for mat, s, p in spec:
+        if mat not in pools:
+            pools[mat] = MaterialPool(mat, 7)
+        jobs.append(SlicePly(mat, s, p, 7, pools[mat]))
+    nops, nitems = record_step(jobs)
+    return torch, tbg, jobs, pools, nops
+
+
+def outputs(jobs, pools):
+    out = [(j.T.cpu().numpy(), j.X.cpu().numpy(), j.wins.cpu().numpy()) for j in jobs]
+    sinks = {m: (p.t_sink.cpu().numpy(), p.x_sink.cpu().numpy()) for m, p in pools.items()}
+    return out, sinks
+
+
+def run(torch, tbg, jobs, pools, mode, cps=2):
+    for p in pools.values():
+        p.t_sink.zero_()
+        p.x_sink.zero_()
+    for j in jobs:
+        j.T.fill_(0xA5)
+        j.X.fill_(0x5A)
+        j.wins.zero_()
+    tbg.batch_tune(cps)
+    tbg.batch_run(mode)
+    tbg.sync()
+    return outputs(jobs, pools), tbg.batch_counts(len(jobs))
+
+
+def test_persistent_equals_plain(setup):
+    torch, tbg, jobs, pools, nops = setup
+    (a, sa), ca = run(torch, tbg, jobs, pools, 0)
+    for cps in (1, 2, 4):
+        (b, sb), cb = run(torch, tbg, jobs, pools, 1, cps)
+        assert ca == cb
+        for x, y in zip(a, b):
+            for u, v in zip(x, y):
+                assert np.array_equal(u, v)
+        for m in sa:
+            assert np.array_equal(sa[m][0], sb[m][0]) and np.array_equal(sa[m][1], sb[m][1])
+
+
+def test_batch_matches_reference(setup):
+    torch, tbg, jobs, pools, nops = setup
+    (b, _), counts = run(torch, tbg, jobs, pools, 1)
+    for j, (T, X, W), c in zip(jobs, b, counts):
+        O = orc.Ref(j.material, 8) if orc.ref_available() else orc.Port(j.material)
+        O.set_stub(1)
+        cpu = CpuSlicePly(O, j)
+        cpu.step()
+        assert c == cpu.cnt_w
+        assert np.array_equal(T, cpu.T), f"W of {j.material} slice {j.s}"
+        assert np.array_equal(W, cpu.wins), f"wins of {j.material} slice {j.s}"
+        assert np.array_equal(X, cpu.X), f"L of {j.material} slice {j.s}"
