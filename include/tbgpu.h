@@ -101,6 +101,11 @@ int tbg_set_stream(void *stream);
 /* Seed and modulus (3 or 5) of the 7-piece WDL stub used by tbg_calc_sub. */
 int tbg_set_stub(uint64_t seed, int modulus);
 
+/* Device memory for a C host that binds its own slices (kslice_setup's
+ * alloc_huge, kslice.c:198-227): zero-filled, 256-byte aligned. */
+int tbg_alloc(size_t bytes, void **dev);
+int tbg_free(void *dev);
+
 /* ---- slot map (kslice_slot / kslice_buf / kslice_sub_buf) ------------ */
 
 /* Binds a device bitmap of `bytes` bytes to slice s of the current
@@ -198,6 +203,11 @@ int tbg_batch_counts(uint64_t *out, int n);
 /* Persistent-launch configuration: CTAs per SM, and the iteration bound of
  * a dependency wait (<= 0 keeps the current one). */
 int tbg_batch_tune(int ctas_per_sm, long long spin_limit);
+
+/* dst = a & ~b over `bytes` (a multiple of 16) of explicit device buffers:
+ * kslice_and_not / kslice_sub_and_not (kslice.c:352-368, 481-487) for a
+ * host that keeps its bitmaps outside the slot map. */
+int tbg_bitmap_and_not(void *dst, const void *a, const void *b, size_t bytes);
 
 /* Waits (bounded: timeout_ms, 0 = 600000) for the stream; reports a kernel
  * status word (TBG_ERR_DEVICE) if one was raised since the last wait. */

@@ -61,6 +61,7 @@ int harness_probe_wdl(Position *pos, int alpha, int beta)
 {
   (void)alpha;
   (void)beta;
+  if (pos->num == 2) return 0;  /* KvK, as probe_table (probe.c:1525) */
   uint64_t key = pos->stm ? H_STM_KEY : 0;
   for (int i = 0; i < pos->num; i++)
     key ^= h_mix64((((uint64_t)pos->pt[i] << 6) | pos->sq[i]) * H_GAMMA

@@ -660,6 +660,7 @@ uint64_t orc_mix64(uint64_t z)
 int orc_stub_value(uint64_t seed, int modulus, const uint8_t *pt,
                    const uint8_t *sq, int num, int stm)
 {
+  if (num == 2) return 0;  /* KvK, as probe_table (probe.c:1525) */
   uint64_t key = stm ? STM_KEY : 0;
   for (int i = 0; i < num; i++)
     key ^= orc_mix64((((uint64_t)pt[i] << 6) | sq[i]) * GAMMA + GAMMA);

@@ -37,8 +37,27 @@ def newest_input_mtime() -> float:
     return t
 
 
+HOST_SRC = os.path.join(HERE, "host", "tbgen.c")
+HOST_OUT = os.path.join(HERE, "tbgen")
+
+
+def build_host(force: bool = False) -> str:
+    """The C host driver (host/tbgen.c), linked against libtbgpu.so."""
+    if not force and os.path.exists(HOST_OUT) and \
+            os.path.getmtime(HOST_OUT) >= max(os.path.getmtime(HOST_SRC), os.path.getmtime(OUT)):
+        return HOST_OUT
+    cmd = ["gcc", "-std=c11", "-O2", "-Wall", "-o", HOST_OUT, HOST_SRC, "-L" + HERE, "-ltbgpu",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("gcc failed building tbgen")
+    return HOST_OUT
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest_input_mtime():
+        build_host()
         return OUT
     cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
     if verbose:
@@ -49,6 +68,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("nvcc failed building libtbgpu.so")
     if verbose:
         sys.stderr.write(r.stderr)
+    build_host(force=True)
     return OUT
 
 

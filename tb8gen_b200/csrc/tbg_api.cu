@@ -948,3 +948,40 @@ extern "C" int tbg_batch_counts(uint64_t *out, int n) {
   CK(cudaMemcpy(out, b.d_counts, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   return TBG_OK;
 }
+
+extern "C" int tbg_alloc(size_t bytes, void **dev) {
+  if (!dev || bytes == 0) return fail(TBG_ERR_ARG, "bad allocation request");
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  *dev = nullptr;
+  cudaError_t e = cudaMalloc(dev, bytes);
+  if (e != cudaSuccess) return fail(TBG_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  CK(cudaMemset(*dev, 0, bytes));
+  return TBG_OK;
+}
+
+extern "C" int tbg_free(void *dev) {
+  if (!dev) return TBG_OK;
+  CK(cudaFree(dev));
+  return TBG_OK;
+}
+
+namespace tbg {
+__global__ void __launch_bounds__(kThreads) k_and_not3(uint4 *d, const uint4 *a, const uint4 *b,
+                                                       uint64_t n16) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n16;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 x = a[i], y = b[i];
+    d[i] = make_uint4(x.x & ~y.x, x.y & ~y.y, x.z & ~y.z, x.w & ~y.w);
+  }
+}
+}  // namespace tbg
+
+extern "C" int tbg_bitmap_and_not(void *dst, const void *a, const void *b, size_t bytes) {
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  if (!dst || !a || !b || !aligned16(dst) || !aligned16(a) || !aligned16(b) || (bytes & 15))
+    return fail(TBG_ERR_ARG, "bad buffers");
+  uint64_t n16 = bytes / 16;
+  k_and_not3<<<g_eng.grid_for((n16 + kThreads - 1) / kThreads, 8), kThreads, 0, g_eng.stream>>>(
+      static_cast<uint4 *>(dst), static_cast<const uint4 *>(a), static_cast<const uint4 *>(b), n16);
+  return g_eng.check_launch("k_and_not3");
+}

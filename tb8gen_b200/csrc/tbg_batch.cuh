@@ -19,7 +19,7 @@
 namespace tbg {
 
 #ifndef TBG_MINB_BATCH
-#define TBG_MINB_BATCH 2
+#define TBG_MINB_BATCH 4
 #endif
 
 __device__ __forceinline__ unsigned int load_acquire(const unsigned int *p) {

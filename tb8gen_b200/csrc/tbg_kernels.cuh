@@ -774,7 +774,8 @@ __global__ void __launch_bounds__(kThreads, TBG_MINB_VERIFY) k_check_successors(
 // ------------------------------------------------ dense per-position kernels
 // Seeded 7-piece WDL stub standing in for probe_wdl (probe.c:1677):
 // VALS[mix64(seed ^ key7) % modulus] with key7 the XOR over the pieces of
-// mix64(((type << 6) | sq) * GAMMA + GAMMA), ^ STM_KEY with black to move.
+// mix64(((type << 6) | sq) * GAMMA + GAMMA), ^ STM_KEY with black to move;
+// bare kings are a draw, as probe_table has it.
 constexpr uint64_t kGamma = 0x9e3779b97f4a7c15ull;
 constexpr uint64_t kStmKey = 0xd1b54a32d192ed03ull;
 
@@ -784,6 +785,8 @@ __device__ __forceinline__ uint64_t piece_key(int type, int sq) {
 
 template <int NS>
 __device__ __forceinline__ int stub_wdl(const DMat &M, const bb *set, int k0, int k1, int stm) {
+  // A capture that leaves the two kings alone is a draw (KvK, probe.c:1525).
+  if (M.num == 3) return 0;
   uint64_t key = stm ? kStmKey : 0;
   key ^= piece_key(M.king_type[0], k0) ^ piece_key(M.king_type[1], k1);
 #pragma unroll
