@@ -237,6 +237,66 @@ int tbg_epilogue_W_static(void *dev_T, const void *dev_wins_in, void *dev_wins_o
                           uint64_t nbits, uint64_t bytes, void *stream,
                           uint64_t *cnt);
 
+/* ---- 7-piece WDL table probes --------------------------------------- */
+
+/* A probe query: the squares of the position's pieces, in the material's
+ * piece order (the order of main(), tb8gen.c:1331-1339: white king, black
+ * king, then knights, bishops, rooks, queens, each type white before
+ * black), and the side to move (0 white, 1 black).  16 bytes, like the
+ * reference Position's sq[]/stm fields (movegen.h) that probe_table reads. */
+typedef struct {
+  uint8_t sq[8];
+  uint8_t stm;
+  uint8_t pad[7];
+} tbg_query;
+
+/* Builds the synthetic WDL table of a pawnless material in the reference's
+ * .rtbw layout, as init_table (probe.c:1210-1344) parses it: magic,
+ * split flag, per-side piece header, setup_pairs bytes (rANS, 64 KiB
+ * blocks, idx_bits 16), frequency table (write_freq_table, rans.c:239-276),
+ * sympat, index table, size table, 64-byte aligned rANS blocks.  Position
+ * idx of side bside holds wdl = VALS[splitmix64(seed ^ idx ^ bside << 63)
+ * mod modulus], VALS = {-2, 0, 2} (modulus 3) or {-2..2} (modulus 5).
+ * The reference has no table writer; this is the writer its reader reads.
+ * on_device != 0: *table is device memory (cudaMalloc; release it with
+ * tbg_free), built by kernels; else host memory (tbg_table_free_host),
+ * built on the CPU for small materials.  *bytes is the file size. */
+int tbg_table_build(const char *material, uint64_t seed, int modulus, int on_device,
+                    void **table, uint64_t *bytes);
+int tbg_table_free_host(void *table);
+
+/* Opens a table image resident in device memory (the reference maps the
+ * file, map_tb / init_table, probe.c:107, 1210).  At most 8 open tables.
+ * Only rANS-compressed pawnless WDL tables are read (the format of
+ * tbg_table_build); other layouts return TBG_ERR_ARG. */
+int tbg_probe_open(const void *dev_table, uint64_t bytes, const char *material, int *handle);
+int tbg_probe_close(int handle);
+
+/* probe_table(pos, 0, WDL) (probe.c:1522-1597) for n device-resident
+ * queries: dev_out[i] = the table's wdl (-2..2) of query i.
+ * mode 0: queries grouped by rANS block, each touched block decoded once
+ * (falls back to mode 1 for tables whose symbols cover unequal position
+ * counts); mode 1: each query decoded on its own, as decompress_rans
+ * (probe.c:1346-1390) does.  Both give identical results. */
+int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t n, void *dev_out, int mode);
+
+/* encode_piece (probe.c:696) after list_squares (probe.c:1511) for n
+ * queries: table index and table side (dev_side may be NULL). */
+int tbg_encode_batch(int handle, const void *dev_queries, uint64_t n, uint64_t *dev_idx,
+                     uint8_t *dev_side);
+
+/* decode_piece (probe.c:1022) for the table's PIECE_ENC layout: the squares,
+ * in table piece order (8 bytes per index), of the positions at indices
+ * dev_idx[] of side `side`. */
+int tbg_decode_batch(int handle, int side, const uint64_t *dev_idx, uint64_t n,
+                     uint8_t *dev_squares);
+
+/* n seeded random legal positions of a material (distinct squares, side
+ * not to move not in check) as queries.  *failed counts queries for which
+ * 64 draws found no legal position (their squares are the last draw). */
+int tbg_gen_positions(const char *material, uint64_t seed, uint64_t n, void *dev_queries,
+                      uint32_t *failed);
+
 /* ---- synthetic inputs (no counterpart in the reference) -------------- */
 
 /* Seeded Bernoulli bitmap: bit i < nbits set iff the (i+1)-th output of the

@@ -73,6 +73,16 @@ def lib():
             "tbg_batch_run": [i],
             "tbg_batch_counts": [C.POINTER(u64), i],
             "tbg_batch_tune": [i, C.c_longlong],
+            "tbg_table_build": [C.c_char_p, u64, i, i, C.POINTER(vp), C.POINTER(u64)],
+            "tbg_table_free_host": [vp],
+            "tbg_probe_open": [vp, u64, C.c_char_p, C.POINTER(i)],
+            "tbg_probe_close": [i],
+            "tbg_probe_wdl_batch": [i, vp, u64, vp, i],
+            "tbg_encode_batch": [i, vp, u64, vp, vp],
+            "tbg_decode_batch": [i, i, vp, u64, vp],
+            "tbg_gen_positions": [C.c_char_p, u64, u64, vp, C.POINTER(C.c_uint32)],
+            "tbg_alloc": [sz, C.POINTER(vp)],
+            "tbg_free": [vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -242,3 +252,74 @@ def batch_counts(n: int):
 
 def batch_tune(ctas_per_sm: int, spin_limit: int = 0):
     check(lib().tbg_batch_tune(ctas_per_sm, spin_limit))
+
+
+# ---------------------------------------------------------------- table probes
+QUERY_BYTES = 16  # tbg_query: sq[8], stm, pad[7]
+
+
+def table_build_host(material: str, seed: int, modulus: int = 3) -> bytes:
+    """The synthetic WDL table of `material`, built on the CPU (small
+    materials): the bytes of the .rtbw file the reference reads."""
+    p, n = C.c_void_p(), C.c_uint64()
+    check(lib().tbg_table_build(material.encode(), seed, modulus, 0, C.byref(p), C.byref(n)))
+    try:
+        return C.string_at(p.value, n.value)
+    finally:
+        lib().tbg_table_free_host(p)
+
+
+class DeviceTable:
+    """A synthetic WDL table built on the device (tbg_table_build) and opened
+    for probing (tbg_probe_open)."""
+
+    def __init__(self, material: str, seed: int, modulus: int = 3, image=None):
+        self.material = material
+        p, n = C.c_void_p(), C.c_uint64()
+        if image is None:
+            check(lib().tbg_table_build(material.encode(), seed, modulus, 1, C.byref(p),
+                                        C.byref(n)))
+            self._owned = p.value
+            self.addr, self.bytes = p.value, n.value
+        else:  # a torch uint8 device tensor holding a table image
+            self._owned = None
+            self._image = image
+            self.addr, self.bytes = image.data_ptr(), image.numel()
+        h = C.c_int()
+        check(lib().tbg_probe_open(C.c_void_p(self.addr), self.bytes, material.encode(),
+                                   C.byref(h)))
+        self.handle = h.value
+
+    def close(self):
+        if self.handle is not None:
+            check(lib().tbg_probe_close(self.handle))
+            self.handle = None
+        if self._owned:
+            check(lib().tbg_free(C.c_void_p(self._owned)))
+            self._owned = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def probe(self, queries, out, mode: int = 0):
+        n = queries.numel() // QUERY_BYTES
+        check(lib().tbg_probe_wdl_batch(self.handle, ptr(queries), n, ptr(out), mode))
+
+    def encode(self, queries, idx, side=None):
+        n = queries.numel() // QUERY_BYTES
+        check(lib().tbg_encode_batch(self.handle, ptr(queries), n, ptr(idx), ptr(side)))
+
+    def decode(self, side: int, idx, squares):
+        check(lib().tbg_decode_batch(self.handle, side, ptr(idx), idx.numel(), ptr(squares)))
+
+
+def gen_positions(material: str, seed: int, queries) -> int:
+    """Fills a uint8 device tensor of n*16 bytes with n seeded legal
+    positions; returns how many draws found no legal position."""
+    failed = C.c_uint32()
+    n = queries.numel() // QUERY_BYTES
+    check(lib().tbg_gen_positions(material.encode(), seed, n, ptr(queries), C.byref(failed)))
+    return failed.value

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libtbgpu.so")
-SOURCES = ["tbg_api.cu", "tbg_noalloc.cu"]
+SOURCES = ["tbg_api.cu", "tbg_noalloc.cu", "tbg_probe_api.cu", "tbg_table.cpp"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
     "-shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-diag-suppress", "550",
@@ -55,19 +55,58 @@ def build_host(force: bool = False) -> str:
     return HOST_OUT
 
 
+OBJ_DIR = os.path.join(HERE, "_build")
+COMPILE_FLAGS = [f for f in NVCC_FLAGS if f != "-shared"]
+
+
+def _obj_current(obj: str) -> bool:
+    """True when obj exists and is newer than every input its .d file lists."""
+    dep = obj + ".d"
+    if not (os.path.exists(obj) and os.path.exists(dep)):
+        return False
+    t = os.path.getmtime(obj)
+    with open(dep) as f:
+        text = f.read().replace("\\\n", " ")
+    inputs = text.split(":", 1)[1].split() if ":" in text else []
+    return all(os.path.exists(i) and os.path.getmtime(i) <= t for i in inputs)
+
+
+def _compile(src: str, verbose: bool, force: bool):
+    obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+    if not force and _obj_current(obj):
+        return obj, None
+    cmd = [nvcc(), *COMPILE_FLAGS, "-MD", "-MF", obj + ".d", "-c", "-o", obj,
+           os.path.join(CSRC, src)]
+    if verbose and src.endswith(".cu"):
+        cmd.insert(1, "-Xptxas=-v")
+    return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source of csrc/ to an object (in parallel) and links
+    libtbgpu.so; rebuilds only when a source or header is newer."""
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest_input_mtime():
         build_host()
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(lambda s: _compile(s, verbose, force), SOURCES))
+    for (obj, r), src in zip(results, SOURCES):
+        if r is None:
+            continue
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed compiling {src}")
+        if verbose:
+            sys.stderr.write(r.stderr)
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT,
+           *[obj for obj, _ in results]]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libtbgpu.so")
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc failed linking libtbgpu.so")
     build_host(force=True)
     return OUT
 
