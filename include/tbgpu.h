@@ -280,6 +280,12 @@ int tbg_probe_close(int handle);
  * (probe.c:1346-1390) does.  Both give identical results. */
 int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t n, void *dev_out, int mode);
 
+/* Device bytes of decoded-symbol scratch a grouped probe may hold (default
+ * 16 GiB).  A touched block takes 16 KiB (codes of at most 256 emitted
+ * symbols) or 32 KiB; blocks beyond the budget are decoded in further
+ * waves.  No counterpart in the reference, which decodes per position. */
+int tbg_probe_tune(uint64_t scratch_bytes);
+
 /* encode_piece (probe.c:696) after list_squares (probe.c:1511) for n
  * queries: table index and table side (dev_side may be NULL). */
 int tbg_encode_batch(int handle, const void *dev_queries, uint64_t n, uint64_t *dev_idx,

@@ -77,6 +77,7 @@ def lib():
             "tbg_table_free_host": [vp],
             "tbg_probe_open": [vp, u64, C.c_char_p, C.POINTER(i)],
             "tbg_probe_close": [i],
+            "tbg_probe_tune": [u64],
             "tbg_probe_wdl_batch": [i, vp, u64, vp, i],
             "tbg_encode_batch": [i, vp, u64, vp, vp],
             "tbg_decode_batch": [i, i, vp, u64, vp],
@@ -314,6 +315,10 @@ class DeviceTable:
 
     def decode(self, side: int, idx, squares):
         check(lib().tbg_decode_batch(self.handle, side, ptr(idx), idx.numel(), ptr(squares)))
+
+
+def probe_tune(scratch_bytes: int):
+    check(lib().tbg_probe_tune(scratch_bytes))
 
 
 def gen_positions(material: str, seed: int, queries) -> int:

@@ -83,24 +83,32 @@ def _compile(src: str, verbose: bool, force: bool):
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compiles every source of csrc/ to an object (in parallel) and links
-    libtbgpu.so; rebuilds only when a source or header is newer."""
-    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest_input_mtime():
-        build_host()
+    """Compiles every source of csrc/ to an object (in parallel, each only
+    when a file it includes is newer) and links libtbgpu.so."""
+    objs = [os.path.join(OBJ_DIR, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+    if not force and not all(os.path.exists(o) for o in objs) and os.path.exists(OUT) and \
+            os.path.getmtime(OUT) >= newest_input_mtime():
+        build_host()  # a library built elsewhere, shipped without its objects
         return OUT
     from concurrent.futures import ThreadPoolExecutor
 
     os.makedirs(OBJ_DIR, exist_ok=True)
     with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         results = list(ex.map(lambda s: _compile(s, verbose, force), SOURCES))
+    compiled = False
     for (obj, r), src in zip(results, SOURCES):
         if r is None:
             continue
+        compiled = True
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"nvcc failed compiling {src}")
         if verbose:
             sys.stderr.write(r.stderr)
+    if not compiled and os.path.exists(OUT) and \
+            os.path.getmtime(OUT) >= max(os.path.getmtime(o) for o in objs):
+        build_host()
+        return OUT
     cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT,
            *[obj for obj, _ in results]]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,15 +1,16 @@
 // WDL probes into rANS-compressed 7-piece tables (probe_table, decompress_rans,
 // probe.c:1346-1390, 1522-1597) and the builder of the synthetic table.
 //
-// A probe batch runs in four passes instead of one independent decode per
+// A probe batch runs in passes instead of one independent decode per
 // position: (1) every position is encoded (encode_piece) and located in its
-// block through the index and size tables; (2) positions are grouped by block
-// (counting sort); (3) every block some position falls in is decoded once, by
-// one thread, from its end down to the lowest position asked for, into a
-// scratch array of symbols; (4) each position reads its symbol and descends
-// the Re-Pair tree to its value.  A 64 KiB block holds up to 65,536 positions,
-// so per-position decoding would cost up to 16,384 rANS steps per probe;
-// grouped, the cost is one decode per touched block.
+// block through the index and size tables, counting the positions per block
+// and the lowest position asked for; (2) a scan numbers the touched blocks;
+// (3) every touched block is decoded once, by one thread, from its end down
+// to the lowest position asked for, into a scratch array of symbol ids;
+// (4) each position reads its symbol and descends the Re-Pair tree to its
+// value.  A 64 KiB block holds up to 65,536 positions, so per-position
+// decoding costs up to 16,384 rANS steps per probe; grouped, the cost is
+// one decode per touched block.
 #pragma once
 
 #include "tbg_device.cuh"
@@ -30,6 +31,7 @@ struct ProbeSide {
   uint32_t key0;            // first block key of this side
   int idx_bits, block_size;
   int sym_positions;        // positions per top-level symbol if all equal, else 0
+  int nsym_emit;            // symbols with nonzero frequency: ids 0 .. nsym_emit-1
 };
 
 struct ProbeTable {
@@ -126,6 +128,33 @@ __device__ __forceinline__ uint8_t descend(const ProbeSide &S, int sym, int lit)
   return S.sympat[3 * sym];
 }
 
+// rans_dec_init / rans_dec_renorm (rans.h:89-95, 129-140) for a block in
+// device memory, whose start is 64-byte aligned so that every word the
+// reader visits is 4-byte aligned: zero words are skipped 64 bytes at a
+// time while the reference's loop would skip all of them, then one at a
+// time under the reference's own condition.
+__device__ __forceinline__ void dev_dec_init(uint64_t &x, const uint8_t *&p, const uint8_t *end) {
+  while (p + 68 < end) {
+    const uint4 *c = reinterpret_cast<const uint4 *>(p);
+    const uint4 a = c[0], b = c[1], d = c[2], e = c[3];
+    if ((a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w | d.x | d.y | d.z | d.w | e.x | e.y | e.z |
+         e.w) != 0)
+      break;
+    p += 64;
+  }
+  while (*reinterpret_cast<const uint32_t *>(p) == 0 && p + 8 < end) p += 4;
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(p);
+  x = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+  p += 8;
+}
+
+__device__ __forceinline__ void dev_dec_renorm(uint64_t &x, const uint8_t *&p) {
+  if (x < kRansL) {
+    x = (x << 32) | *reinterpret_cast<const uint32_t *>(p);
+    p += 4;
+  }
+}
+
 // The whole of decompress_rans for one index (reference path, any table).
 __device__ __forceinline__ int probe_one(const ProbeSide &S, uint64_t idx) {
   uint32_t block;
@@ -136,11 +165,11 @@ __device__ __forceinline__ int probe_one(const ProbeSide &S, uint64_t idx) {
   const uint8_t *p = S.data + ((size_t)block << S.block_size);
   const uint8_t *end = p + ((size_t)1 << S.block_size);
   uint64_t x;
-  rans_dec_init(x, p, end);
+  dev_dec_init(x, p, end);
   int sym = 0;
   for (; lit < 0 && p < end; lit += S.symlen[sym] + 1) {
     sym = rans_dec_get(x, S.entry, S.freq);
-    rans_dec_renorm(x, p);
+    dev_dec_renorm(x, p);
   }
   for (; lit < 0; lit += S.symlen[sym] + 1) sym = rans_dec_get(x, S.entry, S.freq);
   return (int)descend(S, sym, lit) - 2;
@@ -149,6 +178,9 @@ __device__ __forceinline__ int probe_one(const ProbeSide &S, uint64_t idx) {
 // ------------------------------------------------------------ probe passes
 constexpr uint32_t kNoKey = 0xffffffffu;
 
+// Pass 1 of a grouped probe (tables whose symbols all cover L positions):
+// block key and symbol-relative position of every query, per-block counts
+// and lowest position.
 __global__ void k_probe_locate(ProbeTable P, const Query *q, uint64_t n, uint32_t *key,
                                uint32_t *lit, uint32_t *count, uint32_t *minlit, int8_t *out) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
@@ -164,7 +196,11 @@ __global__ void k_probe_locate(ProbeTable P, const Query *q, uint64_t n, uint32_
     uint32_t block;
     int l;
     locate(S, idx, block, l);
-    uint32_t k = S.key0 + block;
+    // counted from the block's first symbol: past the front padding of a
+    // short last block (at most 65535 for any block)
+    const int L = S.sym_positions, npos = block_npos(S, block);
+    l += ((npos + L - 1) / L) * L - npos;
+    const uint32_t k = S.key0 + block;
     key[i] = k;
     lit[i] = (uint32_t)l;
     atomicAdd(&count[k], 1u);
@@ -172,98 +208,235 @@ __global__ void k_probe_locate(ProbeTable P, const Query *q, uint64_t n, uint32_
   }
 }
 
-// Exclusive scan of n counts in one block of 1024 threads (n is at most a
-// few million: the number of blocks of the tables).
-// With kFlag the values scanned are (in[i] != 0).
-template <bool kFlag>
-__global__ void __launch_bounds__(1024) k_scan_exclusive(const uint32_t *in, uint32_t *out,
-                                                         uint64_t n) {
-  __shared__ uint32_t part[1024];
-  const uint64_t per = (n + 1023) / 1024;
-  const uint64_t b0 = threadIdx.x * per, b1 = b0 + per < n ? b0 + per : n;
-  uint32_t s = 0;
-  for (uint64_t i = b0; i < b1; i++) s += kFlag ? (in[i] != 0) : in[i];
-  part[threadIdx.x] = s;
-  __syncthreads();
-  for (int d = 1; d < 1024; d <<= 1) {
-    uint32_t v = threadIdx.x >= d ? part[threadIdx.x - d] : 0;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
-  }
-  uint32_t run = part[threadIdx.x] - s;
-  for (uint64_t i = b0; i < b1; i++) {
-    uint32_t v = kFlag ? (in[i] != 0) : in[i];
-    out[i] = run;
-    run += v;
-  }
-}
+// Exclusive scan of the touched flags (count[k] != 0) of the blocks: tpos[k]
+// is block k's place among the touched blocks, list[tpos[k]] = k for the
+// touched ones.  Three passes over tiles of 4096 keys: tile totals, a scan
+// of the totals, then each tile's scan plus its offset.  The query counts
+// ride along (their total is the number of valid queries).
+constexpr int kScanTile = 4096;
 
-__global__ void k_probe_scatter(const uint32_t *key, uint64_t n, uint32_t *cursor,
-                                uint32_t *order) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    if (key[i] != kNoKey) order[atomicAdd(&cursor[key[i]], 1u)] = (uint32_t)i;
-}
+struct Pair32 {
+  uint32_t a, b;
+};
 
-// Touched blocks, in key order: list[tpos[k]] = k for every k with
-// count > 0, and tq[tpos[k]] = offs[k], the first of k's queries in order[].
-__global__ void k_probe_touched(const uint32_t *count, const uint32_t *tpos, const uint32_t *offs,
-                                uint64_t nkeys, uint32_t *list, uint32_t *tq) {
-  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nkeys;
-       k += (uint64_t)gridDim.x * blockDim.x)
-    if (count[k]) {
-      list[tpos[k]] = (uint32_t)k;
-      tq[tpos[k]] = offs[k];
+// Inclusive scan of (a, b) pairs over the 1024 threads of a block.
+__device__ __forceinline__ Pair32 block_scan(Pair32 v, Pair32 *warp_tot) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t ya = __shfl_up_sync(0xffffffffu, v.a, d), yb = __shfl_up_sync(0xffffffffu, v.b, d);
+    if (lane >= d) {
+      v.a += ya;
+      v.b += yb;
     }
+  }
+  if (lane == 31) warp_tot[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    Pair32 w = warp_tot[lane];
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t ya = __shfl_up_sync(0xffffffffu, w.a, d), yb = __shfl_up_sync(0xffffffffu, w.b, d);
+      if (lane >= d) {
+        w.a += ya;
+        w.b += yb;
+      }
+    }
+    warp_tot[lane] = w;
+  }
+  __syncthreads();
+  if (wid > 0) {
+    v.a += warp_tot[wid - 1].a;
+    v.b += warp_tot[wid - 1].b;
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(const uint32_t *count, uint64_t nkeys,
+                                                      uint32_t *tile_cnt, uint32_t *tile_flag) {
+  __shared__ Pair32 wt[32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + 4 * threadIdx.x;
+  Pair32 v = {0, 0};
+  for (int e = 0; e < 4; e++)
+    if (base + e < nkeys) {
+      const uint32_t c = count[base + e];
+      v.a += c;
+      v.b += c != 0;
+    }
+  v = block_scan(v, wt);
+  if (threadIdx.x == 1023) {
+    tile_cnt[blockIdx.x] = v.a;
+    tile_flag[blockIdx.x] = v.b;
+  }
+}
+
+// Exclusive scan of the tile totals in place (one block; any number of tiles).
+__global__ void __launch_bounds__(1024) k_scan_totals(uint32_t *tile_cnt, uint32_t *tile_flag,
+                                                       uint32_t ntiles) {
+  __shared__ Pair32 wt[32];
+  __shared__ Pair32 carry;
+  if (threadIdx.x == 0) carry = {0, 0};
+  __syncthreads();
+  for (uint32_t t0 = 0; t0 < ntiles; t0 += 1024) {
+    const uint32_t t = t0 + threadIdx.x;
+    Pair32 v = {0, 0};
+    if (t < ntiles) v = {tile_cnt[t], tile_flag[t]};
+    const Pair32 own = v;
+    v = block_scan(v, wt);
+    const Pair32 c = carry;
+    if (t < ntiles) {
+      tile_cnt[t] = c.a + v.a - own.a;
+      tile_flag[t] = c.b + v.b - own.b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = {c.a + v.a, c.b + v.b};
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_finish(const uint32_t *count, uint64_t nkeys,
+                                                       const uint32_t *tile_flag, uint32_t *tpos,
+                                                       uint32_t *list) {
+  __shared__ Pair32 wt[32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + 4 * threadIdx.x;
+  uint32_t c[4];
+  Pair32 v = {0, 0};
+  for (int e = 0; e < 4; e++) {
+    c[e] = base + e < nkeys ? count[base + e] : 0u;
+    v.a += c[e];
+    v.b += c[e] != 0;
+  }
+  const Pair32 own = v;
+  v = block_scan(v, wt);
+  uint32_t rb = tile_flag[blockIdx.x] + v.b - own.b;
+  for (int e = 0; e < 4; e++) {
+    const uint64_t k = base + e;
+    if (k >= nkeys) break;
+    tpos[k] = rb;
+    if (c[e]) list[rb++] = (uint32_t)k;
+  }
 }
 
 __device__ __forceinline__ const ProbeSide &side_of_key(const ProbeTable &P, uint32_t k) {
   return (P.side[1].nblocks && k >= P.side[1].key0) ? P.side[1] : P.side[0];
 }
 
-// One thread per touched block of the wave: decode from the block's end
-// down to the lowest symbol asked for, writing symbol ids in block order.
-__global__ void k_probe_decode(ProbeTable P, const uint32_t *list, uint32_t w0, uint32_t w1,
-                               const uint32_t *minlit, uint16_t *scratch, uint32_t stride) {
-  for (uint32_t t = w0 + blockIdx.x * blockDim.x + threadIdx.x; t < w1;
+// The decode table of one side packed for shared memory, one 64-bit word
+// per bucket b of rans_dec_get (rans.h:111-136): freq of b's own symbol
+// (bits 0-15), freq of its alias (16-31), the alias slot start (32-47), the
+// divider (48-51) and the alias symbol (52-63).
+__device__ __forceinline__ uint64_t pack_bucket(const ProbeSide &S, int b) {
+  const RansEntry e = S.entry[b];
+  const uint32_t a = e.alias_div >> 4;
+  return (uint64_t)S.freq[b] | ((uint64_t)S.freq[a] << 16) | ((uint64_t)e.start << 32) |
+         ((uint64_t)e.alias_div << 48);
+}
+
+// rans_dec_get on a packed bucket table.
+__device__ __forceinline__ int dec_get_packed(uint64_t &x, const uint64_t *tab) {
+  const uint64_t v = x;
+  const int b = (int)((v >> 4) & 4095);
+  uint32_t rem = (uint32_t)(v & 15);
+  const uint64_t e = tab[b];
+  uint32_t f;
+  int sym;
+  if (rem >= (uint32_t)((e >> 48) & 15)) {
+    rem = (rem + (uint32_t)(e >> 32)) & 0xffff;  // wraps by design
+    f = (uint32_t)(e >> 16) & 0xffff;
+    sym = (int)(e >> 52);
+  } else {
+    f = (uint32_t)e & 0xffff;
+    sym = b;
+  }
+  x = (uint64_t)f * (v >> 16) + rem;
+  return sym;
+}
+
+// One thread per touched block of one side: decode from the block's end
+// down to the lowest symbol asked for.  Symbol j of the wave's u-th block
+// goes to scratch[j * W + u] (W blocks in the wave), so that the threads of
+// a warp, which step through j together, store side by side.  TS is uint8_t
+// when every symbol the code emits has an id below 256, else uint16_t.
+//
+// The steps are those of decompress_rans (probe.c:1362-1372): get, then
+// renormalise while the read pointer is inside the block.  Two things are
+// arranged differently: the words renormalisations read come through two
+// 16-byte chunks held in registers, the next one loaded a chunk ahead (its
+// latency hides behind the steps in between), and the pointer test runs
+// once per run of steps that cannot reach the block's end (one step reads
+// at most one word).
+template <typename TS>
+__global__ void __launch_bounds__(256) k_probe_decode(ProbeSide S, const uint32_t *list,
+                                                      uint32_t t0, uint32_t t1, uint32_t wbase,
+                                                      uint32_t W, const uint32_t *minlit,
+                                                      TS *scratch) {
+  __shared__ uint64_t tab[4096];
+  for (int b = threadIdx.x; b < 4096; b += blockDim.x) tab[b] = pack_bucket(S, b);
+  __syncthreads();
+  for (uint32_t t = t0 + blockIdx.x * blockDim.x + threadIdx.x; t < t1;
        t += gridDim.x * blockDim.x) {
     const uint32_t k = list[t];
-    const ProbeSide &S = side_of_key(P, k);
     const uint32_t block = k - S.key0;
     const int L = S.sym_positions;
-    const int npos = block_npos(S, block);
-    const int nsym = (npos + L - 1) / L;
-    const int pad = nsym * L - npos;  // front padding of a short last block
-    const int lo = ((int)minlit[k] + pad) / L;
+    const int nsym = (block_npos(S, block) + L - 1) / L;
+    const int lo = (int)minlit[k] / L;  // positions count from the first symbol
     const uint8_t *p = S.data + ((size_t)block << S.block_size);
     const uint8_t *end = p + ((size_t)1 << S.block_size);
     uint64_t x;
-    rans_dec_init(x, p, end);
-    uint16_t *out = scratch + (size_t)(t - w0) * stride;
-    for (int j = nsym - 1; j >= lo; j--) {
-      out[j] = (uint16_t)rans_dec_get(x, S.entry, S.freq);
-      if (p < end) rans_dec_renorm(x, p);
+    dev_dec_init(x, p, end);
+    // cur: the chunk of the next word (word ci of it); nxt: the chunk after
+    const uint32_t *wp = reinterpret_cast<const uint32_t *>(p);
+    const uint32_t *wend = reinterpret_cast<const uint32_t *>(end);
+    const uint4 *cp = reinterpret_cast<const uint4 *>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(15));
+    const uint4 *cend = reinterpret_cast<const uint4 *>(end);
+    const uint4 zero = make_uint4(0, 0, 0, 0);
+    uint4 cur = cp < cend ? cp[0] : zero;
+    uint4 nxt = cp + 1 < cend ? cp[1] : zero;
+    int ci = (int)((reinterpret_cast<uintptr_t>(p) >> 2) & 3);
+    TS *out = scratch + (size_t)(nsym - 1) * W + (t - wbase);
+    int j = nsym - 1;
+    while (j >= lo) {
+      const int nsafe = (int)(wend - wp);  // renormalisations left inside the block
+      if (nsafe == 0) {
+        for (; j >= lo; j--, out -= W) *out = (TS)dec_get_packed(x, tab);
+        break;
+      }
+      int jstop = j - nsafe;
+      if (jstop < lo - 1) jstop = lo - 1;
+#pragma unroll 2
+      for (; j > jstop; j--, out -= W) {
+        *out = (TS)dec_get_packed(x, tab);
+        if (x < kRansL) {
+          const uint32_t w = ci == 0 ? cur.x : ci == 1 ? cur.y : ci == 2 ? cur.z : cur.w;
+          x = (x << 32) | w;
+          ++wp;
+          if (++ci == 4) {
+            ci = 0;
+            cur = nxt;
+            ++cp;
+            nxt = cp + 1 < cend ? cp[1] : zero;
+          }
+        }
+      }
     }
   }
 }
 
-// One thread per query of the wave's blocks: queries order[tq[w0] ..
-// tq[w1]) (the last wave ends at nvalid, the number of valid queries).
-__global__ void k_probe_answer(ProbeTable P, const uint32_t *order, const uint32_t *tq,
-                               uint32_t w0, uint32_t w1, uint32_t ntouched, uint32_t nvalid,
-                               const uint32_t *key, const uint32_t *lit, const uint32_t *tpos,
-                               const uint16_t *scratch, uint32_t stride, int8_t *out) {
-  const uint32_t q0 = tq[w0], q1 = w1 < ntouched ? tq[w1] : nvalid;
-  for (uint32_t t = q0 + blockIdx.x * blockDim.x + threadIdx.x; t < q1;
-       t += gridDim.x * blockDim.x) {
-    const uint32_t i = order[t];
+// One thread per query: the queries whose block is in the wave (touched
+// blocks w0 .. w0+W-1) read their symbol from the scratch and descend to
+// their value; the others wait for their wave.
+template <typename TS>
+__global__ void k_probe_answer(ProbeTable P, const uint32_t *key, const uint32_t *lit,
+                               const uint32_t *tpos, uint64_t n, uint32_t w0, uint32_t W,
+                               const TS *scratch, int8_t *out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t k = key[i];
+    if (k == kNoKey) continue;
+    const uint32_t u = tpos[k] - w0;
+    if (u >= W) continue;
     const ProbeSide &S = side_of_key(P, k);
     const int L = S.sym_positions;
-    const int npos = block_npos(S, k - S.key0);
-    const int l = (int)lit[i] + ((npos + L - 1) / L) * L - npos;
-    const int sym = scratch[(size_t)(tpos[k] - w0) * stride + l / L];
+    const int l = (int)lit[i];
+    const int sym = scratch[(size_t)(l / L) * W + u];
     out[i] = (int8_t)((int)descend(S, sym, l % L) - 2);
   }
 }

@@ -305,18 +305,16 @@ struct ProbeHandle {
   void *dev_alloc = nullptr;   // decode tables and symlen of both sides
   uint64_t nkeys = 0;
   // scratch, grown on demand
-  uint32_t *key = nullptr, *lit = nullptr, *order = nullptr;
+  uint32_t *key = nullptr, *lit = nullptr;
   uint64_t cap_q = 0;
-  uint32_t *count = nullptr, *minlit = nullptr, *offs = nullptr, *tpos = nullptr, *list = nullptr;
-  uint32_t *tq = nullptr, *cursor = nullptr;
-  uint16_t *symbuf = nullptr;
+  uint32_t *count = nullptr, *minlit = nullptr, *tpos = nullptr, *list = nullptr, *tile = nullptr;
+  uint8_t *symbuf = nullptr;   // decoded symbols (bytes)
   uint64_t cap_sym = 0;
 };
 
 static ProbeHandle g_probe[8];
-// Device bytes of decoded-symbol scratch a grouped probe may hold (blocks
-// decoded per wave = this / 32 KiB).
-static uint64_t g_probe_scratch = 4ull << 30;
+// Device bytes of decoded-symbol scratch a grouped probe may hold.
+static uint64_t g_probe_scratch = 16ull << 30;
 
 static void calc_symlen(std::vector<uint8_t> &len, std::vector<char> &done, const uint8_t *sympat,
                         int s) {
@@ -341,6 +339,8 @@ static int open_table(const uint8_t *dev_table, uint64_t bytes, const char *mate
       break;
     }
   if (h < 0) return fail(TBG_ERR_RANGE, "at most 8 open tables");
+  if (reinterpret_cast<uintptr_t>(dev_table) & 63)
+    return fail(TBG_ERR_ARG, "table image must start on a 64-byte boundary");
   ProbeHandle &H = g_probe[h];
   H = ProbeHandle();
   int rc = spec_from_name(material, H.sp);
@@ -434,6 +434,9 @@ static int open_table(const uint8_t *dev_table, uint64_t bytes, const char *mate
         else same &= L == ps[b].symlen[s];
       }
     S.sym_positions = same && L >= 0 ? L + 1 : 0;
+    S.nsym_emit = 0;
+    for (int s = 0; s < ps[b].num_syms; s++)
+      if (ps[b].dt.freq[s]) S.nsym_emit = s + 1;
   }
   if (sides == 1) H.P.side[1] = ProbeSide();
   H.P.num = num;
@@ -458,6 +461,36 @@ static int grow_buf(T **p, uint64_t *cap, uint64_t n) {
   return TBG_OK;
 }
 
+// Decode and answer in waves of as many touched blocks as the scratch
+// budget holds (TS: the scratch symbol type); usually one wave.
+template <typename TS>
+static int decode_waves(ProbeHandle &H, uint64_t n, int L, uint32_t ntouched, uint32_t nside0,
+                        int8_t *out) {
+  cudaStream_t st = g_eng.stream;
+  const bool two = H.P.side[1].nblocks != 0;
+  const uint64_t per_block = (uint64_t)((kBlockPositions + L - 1) / L) * sizeof(TS);
+  const uint32_t wave =
+      (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntouched, g_probe_scratch / per_block));
+  int rc = grow_buf(&H.symbuf, &H.cap_sym, (uint64_t)wave * per_block);
+  if (rc) return rc;
+  TS *scratch = reinterpret_cast<TS *>(H.symbuf);
+  const int grid = g_eng.num_sms * 8;
+  for (uint32_t w0 = 0; w0 < ntouched; w0 += wave) {
+    const uint32_t w1 = std::min(ntouched, w0 + wave), W = w1 - w0;
+    for (int b = 0; b < (two ? 2 : 1); b++) {
+      const uint32_t t0 = std::max(w0, b ? nside0 : 0u), t1 = std::min(w1, b ? ntouched : nside0);
+      if (t0 >= t1) continue;
+      const uint32_t grid_d = std::min<uint32_t>((t1 - t0 + 255) / 256, g_eng.num_sms * 7);
+      k_probe_decode<TS><<<grid_d, 256, 0, st>>>(H.P.side[b], H.list, t0, t1, w0, W, H.minlit,
+                                                 scratch);
+    }
+    k_probe_answer<TS><<<grid, 256, 0, st>>>(H.P, H.key, H.lit, H.tpos, n, w0, W, scratch, out);
+    rc = g_eng.check_launch("probe decode");
+    if (rc) return rc;
+  }
+  return TBG_OK;
+}
+
 static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, int mode) {
   cudaStream_t st = g_eng.stream;
   const int grid = g_eng.num_sms * 8;
@@ -473,54 +506,39 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
   if ((rc = grow_buf(&H.key, &cap, n))) return rc;
   cap = H.cap_q;
   if ((rc = grow_buf(&H.lit, &cap, n))) return rc;
-  cap = H.cap_q;
-  if ((rc = grow_buf(&H.order, &cap, n))) return rc;
   H.cap_q = std::max(H.cap_q, n);
+  const uint32_t ntiles = (uint32_t)((H.nkeys + kScanTile - 1) / kScanTile);
   if (!H.count) {
     PCK(cudaMalloc(&H.count, H.nkeys * sizeof(uint32_t)));
     PCK(cudaMalloc(&H.minlit, H.nkeys * sizeof(uint32_t)));
-    PCK(cudaMalloc(&H.offs, H.nkeys * sizeof(uint32_t)));
     PCK(cudaMalloc(&H.tpos, H.nkeys * sizeof(uint32_t)));
     PCK(cudaMalloc(&H.list, H.nkeys * sizeof(uint32_t)));
-    PCK(cudaMalloc(&H.tq, H.nkeys * sizeof(uint32_t)));
-    PCK(cudaMalloc(&H.cursor, H.nkeys * sizeof(uint32_t)));
+    PCK(cudaMalloc(&H.tile, 2 * ntiles * sizeof(uint32_t)));
   }
   PCK(cudaMemsetAsync(H.count, 0, H.nkeys * 4, st));
   PCK(cudaMemsetAsync(H.minlit, 0xff, H.nkeys * 4, st));
   k_probe_locate<<<grid, 256, 0, st>>>(H.P, q, n, H.key, H.lit, H.count, H.minlit, out);
-  k_scan_exclusive<false><<<1, 1024, 0, st>>>(H.count, H.offs, H.nkeys);
-  k_scan_exclusive<true><<<1, 1024, 0, st>>>(H.count, H.tpos, H.nkeys);
-  k_probe_touched<<<grid, 256, 0, st>>>(H.count, H.tpos, H.offs, H.nkeys, H.list, H.tq);
-  PCK(cudaMemcpyAsync(H.cursor, H.offs, H.nkeys * 4, cudaMemcpyDeviceToDevice, st));
-  k_probe_scatter<<<grid, 256, 0, st>>>(H.key, n, H.cursor, H.order);
+  k_scan_tiles<<<ntiles, 1024, 0, st>>>(H.count, H.nkeys, H.tile, H.tile + ntiles);
+  k_scan_totals<<<1, 1024, 0, st>>>(H.tile, H.tile + ntiles, ntiles);
+  k_scan_finish<<<ntiles, 1024, 0, st>>>(H.count, H.nkeys, H.tile + ntiles, H.tpos, H.list);
   rc = g_eng.check_launch("probe grouping");
   if (rc) return rc;
-  // touched blocks and valid queries: the last key's scan values
-  uint32_t last[3];
+  // touched blocks (the last key's scan value) and the touched blocks of
+  // side 0 (tpos at side 1's first key)
+  const bool two = H.P.side[1].nblocks != 0;
+  uint32_t last[3] = {0, 0, 0};
   PCK(cudaMemcpyAsync(&last[0], H.tpos + H.nkeys - 1, 4, cudaMemcpyDeviceToHost, st));
   PCK(cudaMemcpyAsync(&last[1], H.count + H.nkeys - 1, 4, cudaMemcpyDeviceToHost, st));
-  PCK(cudaMemcpyAsync(&last[2], H.offs + H.nkeys - 1, 4, cudaMemcpyDeviceToHost, st));
+  if (two) PCK(cudaMemcpyAsync(&last[2], H.tpos + H.P.side[1].key0, 4, cudaMemcpyDeviceToHost, st));
   PCK(cudaStreamSynchronize(st));
   const uint32_t ntouched = last[0] + (last[1] ? 1 : 0);
-  const uint32_t nvalid = last[2] + last[1];
+  const uint32_t nside0 = two ? last[2] : ntouched;
   if (ntouched == 0) return TBG_OK;
   int L = H.P.side[0].sym_positions;
-  if (H.P.side[1].nblocks) L = std::min(L, H.P.side[1].sym_positions);
-  const uint32_t stride = (uint32_t)((kBlockPositions + L - 1) / L);
-  // blocks decoded per wave: as many as the scratch budget holds
-  const uint64_t per_block = (uint64_t)stride * sizeof(uint16_t);
-  const uint32_t wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntouched, g_probe_scratch / per_block));
-  if ((rc = grow_buf(&H.symbuf, &H.cap_sym, (uint64_t)wave * stride))) return rc;
-  for (uint32_t w0 = 0; w0 < ntouched; w0 += wave) {
-    const uint32_t w1 = std::min(ntouched, w0 + wave);
-    k_probe_decode<<<(w1 - w0 + 127) / 128, 128, 0, st>>>(H.P, H.list, w0, w1, H.minlit, H.symbuf,
-                                                          stride);
-    k_probe_answer<<<grid, 256, 0, st>>>(H.P, H.order, H.tq, w0, w1, ntouched, nvalid, H.key, H.lit,
-                                         H.tpos, H.symbuf, stride, out);
-    rc = g_eng.check_launch("probe decode");
-    if (rc) return rc;
-  }
-  return TBG_OK;
+  if (two) L = std::min(L, H.P.side[1].sym_positions);
+  const bool narrow = H.P.side[0].nsym_emit <= 256 && (!two || H.P.side[1].nsym_emit <= 256);
+  return narrow ? decode_waves<uint8_t>(H, n, L, ntouched, nside0, out)
+                : decode_waves<uint16_t>(H, n, L, ntouched, nside0, out);
 }
 
 }  // namespace tbg
@@ -550,9 +568,9 @@ extern "C" int tbg_probe_close(int handle) {
   if (handle < 0 || handle >= 8 || !g_probe[handle].used) return fail(TBG_ERR_ARG, "bad handle");
   ProbeHandle &H = g_probe[handle];
   cudaStreamSynchronize(g_eng.stream);
-  for (void *p : {(void *)H.dev_alloc, (void *)H.key, (void *)H.lit, (void *)H.order, (void *)H.count,
-                  (void *)H.minlit, (void *)H.offs, (void *)H.tpos, (void *)H.list, (void *)H.tq,
-                  (void *)H.cursor, (void *)H.symbuf})
+  for (void *p : {(void *)H.dev_alloc, (void *)H.key, (void *)H.lit, (void *)H.count,
+                  (void *)H.minlit, (void *)H.tpos, (void *)H.list, (void *)H.tile,
+                  (void *)H.symbuf})
     if (p) cudaFree(p);
   H = ProbeHandle();
   return TBG_OK;
@@ -606,4 +624,10 @@ extern "C" int tbg_gen_positions(const char *material, uint64_t seed, uint64_t n
   cudaFree(d_fail);
   if (failed) *failed = f;
   return rc;
+}
+
+extern "C" int tbg_probe_tune(uint64_t scratch_bytes) {
+  if (scratch_bytes < (64u << 10)) return fail(TBG_ERR_ARG, "scratch below 64 KiB");
+  g_probe_scratch = scratch_bytes;
+  return TBG_OK;
 }
