@@ -12,7 +12,13 @@ Workloads (synthetic, seeded; there is no public dataset for this path):
          with p in {0.001, 0.01, 0.05}; neighbour marks go to per-material
          shared bitmaps (see plyjob).
 
-A step is one slice-ply of every slice of the workload.  `value` is the
+  probe  2^28 seeded legal positions (seed 3), half KRRRvKRR, half KQRvKRR,
+         probed (WDL) against the synthetic rANS tables of the two
+         materials (seed 3, values mod 3); a step is one probe batch of all
+         positions, and the index round trip (encode, decode, re-encode) is
+         timed beside it.  Metric: probe positions/s.
+
+A step of the ply workloads is one slice-ply of every slice of the workload.  `value` is the
 positions of all slices (all ranks) per second of device time, inputs
 resident in HBM.  `e2e` is the same metric through the public C ABI with
 the inputs copied from pinned host memory and the W/L results copied back
@@ -44,7 +50,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="slice", choices=["slice", "mix", "small"])
+    ap.add_argument("--workload", default="slice", choices=["slice", "mix", "small", "probe"])
+    ap.add_argument("--probe-n", type=int, default=1 << 28,
+                    help="probe workload: positions per step (split over the materials)")
+    ap.add_argument("--probe-materials", default="KRRRvKRR,KQRvKRR",
+                    help="probe workload: materials (a smaller one makes a profiling case)")
     ap.add_argument("--path", default="batched", choices=["plain", "batched"])
     ap.add_argument("--ctas-per-sm", type=int, default=0,
                     help="persistent-kernel CTAs per SM (0: autotune)")
@@ -137,12 +147,13 @@ def measured_peak():
 
 
 def committed_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/traffic.json, written from an ncu capture), if present."""
+    """DRAM bytes per unit (position, or block for the probe decode) of
+    `kernel` from profiles/traffic.json, which records one ncu capture of a
+    smaller case of the same kernel; None if absent."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             d = json.load(f)
-        return d.get(kernel)
+        return float(d[kernel]["bytes_per_unit"])
     except Exception:
         return None
 
@@ -278,7 +289,8 @@ def run_engine(a, rank, world, local):
         ph = max(phase_ms, key=phase_ms.get)
         dom, dom_ms, alg = kname[ph], phase_ms[ph], per_pos[ph] * positions
     achieved = alg / (dom_ms / 1e3) / 1e9
-    traffic = committed_traffic(dom)
+    tr = committed_traffic(dom)
+    traffic = int(tr * positions) if tr else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "alg_bytes_per_launch": int(alg), "traffic": traffic,
@@ -439,6 +451,359 @@ def run_reference(a, rank, world, local):
     }
 
 
+# ------------------------------------------------------------ probe workload
+PROBE_METRIC = "probe positions/s (bit-exact)"
+PROBE_MATS = ("KRRRvKRR", "KQRvKRR")
+PROBE_SEED = 3
+PROBE_BLOCK = 65536
+
+
+class ProbeSet:
+    """The probe workload on the device: the synthetic table and the seeded
+    positions (and result buffer) of each material."""
+
+    def __init__(self, n_total, rank=0, materials=PROBE_MATS):
+        import torch
+
+        import tb8gen_b200 as tbg
+
+        self.items = []
+        self.materials = tuple(materials)
+        per = n_total // len(self.materials)
+        for m in self.materials:
+            t = tbg.DeviceTable(m, PROBE_SEED, 3)
+            q = torch.empty(per * 16, dtype=torch.uint8, device="cuda")
+            failed = tbg.gen_positions(m, PROBE_SEED + 1000 * rank, q)
+            if failed:
+                raise RuntimeError(f"{failed} draws found no legal {m} position")
+            out = torch.empty(per, dtype=torch.int8, device="cuda")
+            self.items.append((m, t, q, out))
+        self.positions = per * len(self.materials)
+        self.table_bytes = sum(t.bytes for _, t, _, _ in self.items)
+
+    def probe(self):
+        for _, t, q, out in self.items:
+            t.probe(q, out, 0)
+
+    def close(self):
+        for _, t, _, _ in self.items:
+            t.close()
+
+
+def probe_roundtrip(m, t, q):
+    """encode -> decode -> re-encode of every query on the device; returns
+    the number of indices that did not come back.  Both sides of these
+    tables list their pieces in one order, so side 0's decode serves both;
+    the decoded squares are re-encoded with the side to move of the table
+    side (a symmetric table keeps black-to-move positions colour-flipped)."""
+    import torch
+
+    import tb8gen_b200 as tbg
+
+    n = q.numel() // 16
+    idx = torch.empty(n, dtype=torch.int64, device="cuda")
+    side = torch.empty(n, dtype=torch.uint8, device="cuda")
+    t.encode(q, idx, side)
+    sq = torch.empty((n, 8), dtype=torch.uint8, device="cuda")
+    t.decode(0, idx, sq)
+    cols = tbg.table_to_query_columns(m)
+    q2 = torch.zeros((n, 16), dtype=torch.uint8, device="cuda")
+    q2[:, :len(cols)] = sq[:, cols]
+    q2[:, 8] = side
+    idx2 = torch.empty_like(idx)
+    t.encode(q2.view(-1), idx2)
+    return int((idx2 != idx).sum().item())
+
+
+def write_sparse_tables(ps, per_mat, directory):
+    """Table files for the reference's reader holding what a sample of the
+    first `per_mat` queries of each material reads: the front of the image
+    (header, code, index and size tables) and the touched blocks; the rest
+    of each file is a hole.  Returns the host queries of the samples."""
+    import torch
+
+    import tb8gen_b200 as tbg
+    from oracle import probe_ref as PR
+
+    samples = []
+    for m, t, q, _ in ps.items:
+        qs = q[: per_mat * 16]
+        n = qs.numel() // 16
+        idx = torch.empty(n, dtype=torch.int64, device="cuda")
+        side = torch.empty(n, dtype=torch.uint8, device="cuda")
+        t.encode(qs, idx, side)
+        img = t.image()
+        path = os.path.join(directory, PR.table_file_name(m) + ".rtbw")
+        sides = [0]
+        try:
+            t.layout(1)
+            sides.append(1)
+        except tbg.TbgError:
+            pass  # a symmetric material: one side
+        with open(path, "wb") as f:
+            f.truncate(t.bytes)
+            off0 = t.layout(0)[0]
+            f.seek(0)
+            f.write(img[:off0].cpu().numpy().tobytes())
+            for b in sides:
+                off, nb, _ = t.layout(b)
+                blk = torch.unique((idx[side == b] >> 16))
+                if blk.numel() == 0:
+                    continue
+                data = img[off: off + nb * PROBE_BLOCK].view(nb, PROBE_BLOCK)
+                rows = data.index_select(0, blk).cpu().numpy()
+                for k, row in zip(blk.cpu().numpy().tolist(), rows):
+                    f.seek(off + k * PROBE_BLOCK)
+                    f.write(row.tobytes())
+        samples.append((m, qs.cpu().numpy().reshape(n, 16)))
+    return samples
+
+
+def time_reference_probe(directory, samples, seconds, threads):
+    """The reference's probe_table (oracle/_ref/libtbprobe.so) over the
+    samples on `threads` host threads, repeated until `seconds` pass;
+    returns (positions/s, passes, results of the first pass)."""
+    import threading
+
+    import numpy as np
+
+    from oracle import probe_ref as PR
+
+    ref = PR.RefProbe(directory)
+    if ref.found != len(samples):
+        raise RuntimeError(f"reference found {ref.found} tables")
+    first = {m: ref.probe(m, q) for m, q in samples}  # maps the tables, warms the page cache
+    chunks = []
+    for m, q in samples:
+        pt = np.array(PR.material_pieces(m), dtype=np.uint8)
+        for part in np.array_split(np.arange(len(q)), threads):
+            if len(part):
+                chunks.append((pt, np.ascontiguousarray(q[part]), np.zeros(len(part), np.int8)))
+    import ctypes as C
+    L = PR.probe_lib()
+    total = sum(len(c[1]) for c in chunks)
+    passes, t0 = 0, time.perf_counter()
+    while True:
+        per_thread = [chunks[i::threads] for i in range(threads)]
+
+        def work(lst):
+            for pt, qq, oo in lst:
+                L.refp_probe(C.c_void_p(pt.ctypes.data), len(pt), C.c_void_p(qq.ctypes.data),
+                             len(qq), C.c_void_p(oo.ctypes.data))
+        ths = [threading.Thread(target=work, args=(lst,)) for lst in per_thread]
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        passes += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return total * passes / el, passes, first
+
+
+def probe_cpu_baseline(ps, seconds, per_mat=8192):
+    import shutil
+    import tempfile
+
+    threads = os.cpu_count() or 1
+    d = tempfile.mkdtemp(prefix="tbprobe_")
+    try:
+        samples = write_sparse_tables(ps, per_mat, d)
+        v, passes, first = time_reference_probe(d, samples, seconds, threads)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    # the engine's answers for the same positions, bit for bit
+    match = all(bool((first[m] == out[:per_mat].cpu().numpy()).all())
+                for m, _, _, out in ps.items)
+    return {"value": round(v, 1), "unit": "positions/s", "cores": threads, "kind": "reference",
+            "sample": (f"the first {per_mat} positions of each material ({len(samples) * per_mat} "
+                       f"probes) through the reference's probe_table on {threads} threads, "
+                       f"{passes} passes; tables as sparse files holding the touched blocks"),
+            "sample_bit_exact": match}
+
+
+def run_probe(a, rank, world, local):
+    import torch
+
+    import tb8gen_b200 as tbg
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    tbg.init()
+    tbg.set_stream(stream)
+    t0 = time.time()
+    ps = ProbeSet(a.probe_n, rank, a.probe_materials.split(","))
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
+    for _ in range(a.warmup):
+        ps.probe()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = tbg.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    phases = []
+    for _ in range(a.steps):
+        ps.probe()
+        phases.append([t.phase_ms() for _, t, _, _ in ps.items])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = tbg.launches() - n0
+    ms = e0.elapsed_time(e1) / a.steps
+    clk = clocks.stop()
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = ps.positions * world / (ms / 1e3)
+
+    # dominant kernel: the block decode (k_probe_decode), one touched block =
+    # 64 KiB read; its device time from the library's events
+    dec_ms = statistics.median(sum(p[0][1] for p in step) for step in phases)
+    touched = sum(p[1] for p in phases[-1])
+    alg = touched * PROBE_BLOCK
+    peak, peak_kind = measured_peak()
+    achieved = alg / (dec_ms / 1e3) / 1e9
+    tr = committed_traffic("k_probe_decode")
+    roofline = {"bound": "hbm", "kernel": "k_probe_decode", "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "peak_source": peak_kind, "alg_bytes_per_launch": alg,
+                "traffic": int(tr * touched) if tr else None,
+                "note": "algorithmic bytes = touched blocks x 64 KiB (each read once); "
+                        "the rANS steps, not HBM, bound this kernel"}
+    phase = {m: {"locate_ms": round(statistics.median(s[i][0][0] for s in phases), 3),
+                 "decode_ms": round(statistics.median(s[i][0][1] for s in phases), 3),
+                 "answer_ms": round(statistics.median(s[i][0][2] for s in phases), 3),
+                 "touched_blocks": phases[-1][i][1]}
+             for i, (m, _, _, _) in enumerate(ps.items)}
+
+    # index round trip (encode, decode, re-encode) of every position
+    r0 = torch.cuda.Event(enable_timing=True)
+    r1 = torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    bad = sum(probe_roundtrip(m, t, q) for m, t, q, _ in ps.items)
+    r1.record(stream)
+    torch.cuda.synchronize()
+    rt_ms = r0.elapsed_time(r1)
+
+    e2e = None
+    if not a.no_e2e:
+        e2e = run_probe_e2e(a, ps, stream)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = probe_cpu_baseline(ps, min(a.cpu_seconds, 20.0))
+    line = {
+        "metric": PROBE_METRIC, "value": round(value, 1), "unit": "positions/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded legal positions, seeded synthetic rANS tables)",
+        "config": {"workload": "probe", "materials": list(ps.materials),
+                   "positions_per_step": ps.positions, "table_bytes": ps.table_bytes,
+                   "block_bytes": PROBE_BLOCK, "seed": PROBE_SEED,
+                   "l2": f"inputs larger than L2 ({ps.table_bytes / 1e9:.1f} GB of tables, "
+                         f"{ps.positions * 16 / 1e9:.1f} GB of positions)"},
+        "phases": phase, "table_build_s": round(build_s, 2),
+        "index_roundtrip": {"ms": round(rt_ms, 3),
+                            "positions_per_s": round(ps.positions / (rt_ms / 1e3), 1),
+                            "mismatches": bad},
+        "roofline": roofline, "gpu_launches": launches, "clocks": clk, "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    ps.close()
+    return line
+
+
+def run_probe_e2e(a, ps, stream):
+    """Probe batches through the C ABI from pinned host memory: per step the
+    H2D copy of every query and the D2H copy of every result."""
+    import torch
+
+    hq = [torch.empty(q.numel(), dtype=torch.uint8, pin_memory=True) for _, _, q, _ in ps.items]
+    ho = [torch.empty(o.numel(), dtype=torch.int8, pin_memory=True) for _, _, _, o in ps.items]
+    for h, (_, _, q, _) in zip(hq, ps.items):
+        h.copy_(q)
+    torch.cuda.synchronize()
+
+    def one():
+        for h, r, (_, t, q, out) in zip(hq, ho, ps.items):
+            q.copy_(h, non_blocking=True)
+            t.probe(q, out, 0)
+            r.copy_(out, non_blocking=True)
+
+    one()
+    torch.cuda.synchronize()
+    steps = max(2, min(a.steps, 5))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": round(ps.positions / (ms / 1e3), 1), "unit": "positions/s",
+            "ms_per_step": round(ms, 3), "h2d_bytes_per_step": sum(h.numel() for h in hq),
+            "d2h_bytes_per_step": sum(r.numel() for r in ho), "steps": steps}
+
+
+def run_probe_reference(a, rank, world, local):
+    """Reference arm of the probe workload: the reference's probe_table on
+    all host cores.  The tables and positions are made on the device (the
+    reference has no table writer); only the reference's CPU probe is timed,
+    one pass over a 16,384-position sample per step."""
+    if rank != 0:
+        return None
+    import shutil
+    import tempfile
+
+    import torch
+
+    import tb8gen_b200 as tbg
+
+    torch.cuda.set_device(local)
+    tbg.init()
+    ps = ProbeSet(a.probe_n, 0, a.probe_materials.split(","))
+    per_mat = 8192
+    threads = os.cpu_count() or 1
+    d = tempfile.mkdtemp(prefix="tbprobe_")
+    try:
+        samples = write_sparse_tables(ps, per_mat, d)
+        per_step = []
+        for _ in range(a.warmup + a.steps):
+            v, _, _ = time_reference_probe(d, samples, 0.0, threads)
+            per_step.append(v)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+        ps.close()
+    v = statistics.median(per_step[a.warmup:] or per_step)
+    n = per_mat * len(ps.materials)
+    return {
+        "metric": PROBE_METRIC, "value": round(v, 1), "unit": "positions/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(n / v * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded legal positions, seeded synthetic rANS tables)",
+        "config": {"workload": "probe", "materials": list(ps.materials),
+                   "positions_per_step": n, "note": "a step is one pass over the sample"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(v, 1), "unit": "positions/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{per_mat} positions of each material per step, "
+                                   f"probe_table on {threads} threads"},
+        "e2e": {"value": round(v, 1), "unit": "positions/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
 def main():
     a = parse()
     rank, world, local = dist_env()
@@ -450,7 +815,10 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        if a.impl == "reference":
+        if a.workload == "probe":
+            line = (run_probe_reference if a.impl == "reference" else run_probe)(a, rank, world,
+                                                                                  local)
+        elif a.impl == "reference":
             line = run_reference(a, rank, world, local)
         else:
             line = run_engine(a, rank, world, local)

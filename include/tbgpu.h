@@ -280,6 +280,19 @@ int tbg_probe_close(int handle);
  * (probe.c:1346-1390) does.  Both give identical results. */
 int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t n, void *dev_out, int mode);
 
+/* Where side `side` of an open table keeps its rANS blocks: byte offset of
+ * block 0 in the image (block k at data_offset + k * 65536), the number of
+ * blocks and of positions (init_table's walk, probe.c:1304-1331). */
+int tbg_probe_layout(int handle, int side, uint64_t *data_offset, uint64_t *nblocks,
+                     uint64_t *positions);
+
+/* Device time of the phases of the handle's last grouped batch (CUDA
+ * events on the library's stream): ms[0] locate and scan, ms[1] the block
+ * decodes, ms[2] the answers; *touched_blocks (may be NULL) the blocks it
+ * decoded.  With several decode waves, ms[1] also holds the answers of the
+ * earlier waves.  Waits for the batch to finish. */
+int tbg_probe_phase_ms(int handle, float ms[3], uint64_t *touched_blocks);
+
 /* Device bytes of decoded-symbol scratch a grouped probe may hold (default
  * 16 GiB).  A touched block takes 16 KiB (codes of at most 256 emitted
  * symbols) or 32 KiB; blocks beyond the budget are decoded in further

@@ -98,8 +98,21 @@ class RefProbe:
     """The reference's probe over the tables of one directory."""
 
     def __init__(self, directory: str):
+        import sys
+
         self.L = probe_lib()
-        self.found = self.L.refp_init(directory.encode())
+        # init_tablebases prints a count line on stdout; keep stdout clean for
+        # callers that print one result line there
+        sys.stdout.flush()
+        saved = os.dup(1)
+        try:
+            with open(os.devnull, "w") as null:
+                os.dup2(null.fileno(), 1)
+                self.found = self.L.refp_init(directory.encode())
+                C.CDLL(None).fflush(None)
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
 
     @staticmethod
     def _pt(material: str) -> np.ndarray:

@@ -78,6 +78,8 @@ def lib():
             "tbg_probe_open": [vp, u64, C.c_char_p, C.POINTER(i)],
             "tbg_probe_close": [i],
             "tbg_probe_tune": [u64],
+            "tbg_probe_phase_ms": [i, C.POINTER(C.c_float), C.POINTER(u64)],
+            "tbg_probe_layout": [i, i, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)],
             "tbg_probe_wdl_batch": [i, vp, u64, vp, i],
             "tbg_encode_batch": [i, vp, u64, vp, vp],
             "tbg_decode_batch": [i, i, vp, u64, vp],
@@ -305,6 +307,31 @@ class DeviceTable:
     def __exit__(self, *exc):
         self.close()
 
+    def layout(self, side: int):
+        """(data offset, blocks, positions) of one side of the table."""
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(lib().tbg_probe_layout(self.handle, side, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def phase_ms(self):
+        """((locate, decode, answer) device ms, touched blocks) of the last
+        grouped batch."""
+        ms = (C.c_float * 3)()
+        nb = C.c_uint64()
+        check(lib().tbg_probe_phase_ms(self.handle, ms, C.byref(nb)))
+        return tuple(ms), nb.value
+
+    def image(self):
+        """The table image as a uint8 torch tensor on the device (a view)."""
+        import torch
+
+        addr, nbytes = self.addr, self.bytes
+
+        class _Arr:
+            __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1",
+                                        "data": (addr, False), "version": 3}
+        return torch.as_tensor(_Arr(), device="cuda")
+
     def probe(self, queries, out, mode: int = 0):
         n = queries.numel() // QUERY_BYTES
         check(lib().tbg_probe_wdl_batch(self.handle, ptr(queries), n, ptr(out), mode))
@@ -319,6 +346,47 @@ class DeviceTable:
 
 def probe_tune(scratch_bytes: int):
     check(lib().tbg_probe_tune(scratch_bytes))
+
+
+_PIECE_RANK = {6: 1, 14: 2, 2: 3, 10: 4, 3: 5, 11: 6, 4: 7, 12: 8, 5: 9, 13: 10}
+
+
+def material_pieces(material: str) -> list[int]:
+    """Piece codes (type | 8 for black) in main()'s order (tb8gen.c:1331-1339):
+    the order of a query's squares."""
+    pt, black = [], 0
+    for ch in material:
+        if ch == "v":
+            black = 8
+            continue
+        pt.append(("PNBRQK".index(ch) + 1) | black)
+    return sorted(pt, key=lambda p: _PIECE_RANK[p])
+
+
+def table_pieces(material: str) -> list[int]:
+    """The piece order of the synthetic tables (tbg_table_build): the kings,
+    then, unless only the kings are unique, the first other unique piece,
+    then the rest in material order.  tbg_decode_batch lists squares so."""
+    pt = material_pieces(material)
+    cnt = {p: pt.count(p) for p in pt}
+    out, rest = pt[:2], list(pt[2:])
+    if sum(1 for p in cnt if cnt[p] == 1) > 2:
+        u = next(p for p in rest if cnt[p] == 1)
+        out.append(u)
+        rest.remove(u)
+    return out + rest
+
+
+def table_to_query_columns(material: str) -> list[int]:
+    """cols[j] = the table-order column holding the square of query column j."""
+    tp, mp = table_pieces(material), material_pieces(material)
+    used = [False] * len(tp)
+    cols = []
+    for p in mp:
+        k = next(k for k in range(len(tp)) if tp[k] == p and not used[k])
+        used[k] = True
+        cols.append(k)
+    return cols
 
 
 def gen_positions(material: str, seed: int, queries) -> int:

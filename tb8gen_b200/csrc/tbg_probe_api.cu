@@ -302,6 +302,7 @@ struct ProbeHandle {
   bool used = false;
   ProbeTable P;
   Spec sp;
+  const uint8_t *base = nullptr;  // the table image
   void *dev_alloc = nullptr;   // decode tables and symlen of both sides
   uint64_t nkeys = 0;
   // scratch, grown on demand
@@ -310,6 +311,11 @@ struct ProbeHandle {
   uint32_t *count = nullptr, *minlit = nullptr, *tpos = nullptr, *list = nullptr, *tile = nullptr;
   uint8_t *symbuf = nullptr;   // decoded symbols (bytes)
   uint64_t cap_sym = 0;
+  // events of the last grouped batch: start, first decode, after the last
+  // decode, end
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool timed = false;
+  uint64_t touched = 0;        // blocks decoded by the last grouped batch
 };
 
 static ProbeHandle g_probe[8];
@@ -343,6 +349,7 @@ static int open_table(const uint8_t *dev_table, uint64_t bytes, const char *mate
     return fail(TBG_ERR_ARG, "table image must start on a 64-byte boundary");
   ProbeHandle &H = g_probe[h];
   H = ProbeHandle();
+  H.base = dev_table;
   int rc = spec_from_name(material, H.sp);
   if (rc) return rc;
   rc = enc_tables_device();
@@ -475,6 +482,7 @@ static int decode_waves(ProbeHandle &H, uint64_t n, int L, uint32_t ntouched, ui
   if (rc) return rc;
   TS *scratch = reinterpret_cast<TS *>(H.symbuf);
   const int grid = g_eng.num_sms * 8;
+  PCK(cudaEventRecord(H.ev[1], st));
   for (uint32_t w0 = 0; w0 < ntouched; w0 += wave) {
     const uint32_t w1 = std::min(ntouched, w0 + wave), W = w1 - w0;
     for (int b = 0; b < (two ? 2 : 1); b++) {
@@ -484,6 +492,7 @@ static int decode_waves(ProbeHandle &H, uint64_t n, int L, uint32_t ntouched, ui
       k_probe_decode<TS><<<grid_d, 256, 0, st>>>(H.P.side[b], H.list, t0, t1, w0, W, H.minlit,
                                                  scratch);
     }
+    if (w1 == ntouched) PCK(cudaEventRecord(H.ev[2], st));
     k_probe_answer<TS><<<grid, 256, 0, st>>>(H.P, H.key, H.lit, H.tpos, n, w0, W, scratch, out);
     rc = g_eng.check_launch("probe decode");
     if (rc) return rc;
@@ -501,6 +510,9 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
     return g_eng.check_launch("k_probe_direct");
   }
   if (n >= (1ull << 32)) return fail(TBG_ERR_RANGE, "batch of 2^32 positions or more");
+  if (!H.ev[0])
+    for (auto &e : H.ev) PCK(cudaEventCreate(&e));
+  H.timed = false;
   int rc;
   uint64_t cap = H.cap_q;
   if ((rc = grow_buf(&H.key, &cap, n))) return rc;
@@ -515,6 +527,7 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
     PCK(cudaMalloc(&H.list, H.nkeys * sizeof(uint32_t)));
     PCK(cudaMalloc(&H.tile, 2 * ntiles * sizeof(uint32_t)));
   }
+  PCK(cudaEventRecord(H.ev[0], st));
   PCK(cudaMemsetAsync(H.count, 0, H.nkeys * 4, st));
   PCK(cudaMemsetAsync(H.minlit, 0xff, H.nkeys * 4, st));
   k_probe_locate<<<grid, 256, 0, st>>>(H.P, q, n, H.key, H.lit, H.count, H.minlit, out);
@@ -533,12 +546,17 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
   PCK(cudaStreamSynchronize(st));
   const uint32_t ntouched = last[0] + (last[1] ? 1 : 0);
   const uint32_t nside0 = two ? last[2] : ntouched;
+  H.touched = ntouched;
   if (ntouched == 0) return TBG_OK;
   int L = H.P.side[0].sym_positions;
   if (two) L = std::min(L, H.P.side[1].sym_positions);
   const bool narrow = H.P.side[0].nsym_emit <= 256 && (!two || H.P.side[1].nsym_emit <= 256);
-  return narrow ? decode_waves<uint8_t>(H, n, L, ntouched, nside0, out)
-                : decode_waves<uint16_t>(H, n, L, ntouched, nside0, out);
+  rc = narrow ? decode_waves<uint8_t>(H, n, L, ntouched, nside0, out)
+              : decode_waves<uint16_t>(H, n, L, ntouched, nside0, out);
+  if (rc) return rc;
+  PCK(cudaEventRecord(H.ev[3], st));
+  H.timed = true;
+  return TBG_OK;
 }
 
 }  // namespace tbg
@@ -568,6 +586,8 @@ extern "C" int tbg_probe_close(int handle) {
   if (handle < 0 || handle >= 8 || !g_probe[handle].used) return fail(TBG_ERR_ARG, "bad handle");
   ProbeHandle &H = g_probe[handle];
   cudaStreamSynchronize(g_eng.stream);
+  for (auto &e : H.ev)
+    if (e) cudaEventDestroy(e);
   for (void *p : {(void *)H.dev_alloc, (void *)H.key, (void *)H.lit, (void *)H.count,
                   (void *)H.minlit, (void *)H.tpos, (void *)H.list, (void *)H.tile,
                   (void *)H.symbuf})
@@ -629,5 +649,30 @@ extern "C" int tbg_gen_positions(const char *material, uint64_t seed, uint64_t n
 extern "C" int tbg_probe_tune(uint64_t scratch_bytes) {
   if (scratch_bytes < (64u << 10)) return fail(TBG_ERR_ARG, "scratch below 64 KiB");
   g_probe_scratch = scratch_bytes;
+  return TBG_OK;
+}
+
+extern "C" int tbg_probe_layout(int handle, int side, uint64_t *data_offset, uint64_t *nblocks,
+                                uint64_t *positions) {
+  if (handle < 0 || handle >= 8 || !g_probe[handle].used || side < 0 || side > 1)
+    return fail(TBG_ERR_ARG, "bad handle/side");
+  const ProbeHandle &H = g_probe[handle];
+  const ProbeSide &S = H.P.side[side];
+  if (side == 1 && !S.nblocks) return fail(TBG_ERR_ARG, "the table has one side");
+  if (data_offset) *data_offset = (uint64_t)(S.data - H.base);
+  if (nblocks) *nblocks = S.nblocks;
+  if (positions) *positions = S.ei.size;
+  return TBG_OK;
+}
+
+extern "C" int tbg_probe_phase_ms(int handle, float ms[3], uint64_t *touched_blocks) {
+  if (handle < 0 || handle >= 8 || !g_probe[handle].used || !ms) return fail(TBG_ERR_ARG, "bad handle");
+  ProbeHandle &H = g_probe[handle];
+  if (!H.timed) return fail(TBG_ERR_STATE, "no grouped batch with touched blocks since the last call");
+  PCK(cudaEventSynchronize(H.ev[3]));
+  PCK(cudaEventElapsedTime(&ms[0], H.ev[0], H.ev[1]));
+  PCK(cudaEventElapsedTime(&ms[1], H.ev[1], H.ev[2]));
+  PCK(cudaEventElapsedTime(&ms[2], H.ev[2], H.ev[3]));
+  if (touched_blocks) *touched_blocks = H.touched;
   return TBG_OK;
 }
