@@ -12,6 +12,10 @@ Workloads (synthetic, seeded; there is no public dataset for this path):
          with p in {0.001, 0.01, 0.05}; neighbour marks go to per-material
          shared bitmaps (see plyjob).
 
+  serve  a seeded Poisson stream (seed 4) of ply jobs (70%) and probe
+         batches (30%, 1k-1M positions) served with continuous batching under
+         an HBM admission budget, swept over arrival rates, beside one
+         request at a time; p50/p99 latency and positions/s.
   probe  2^28 seeded legal positions (seed 3), half KRRRvKRR, half KQRvKRR,
          probed (WDL) against the synthetic rANS tables of the two
          materials (seed 3, values mod 3); a step is one probe batch of all
@@ -50,7 +54,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="slice", choices=["slice", "mix", "small", "probe"])
+    ap.add_argument("--workload", default="slice",
+                    choices=["slice", "mix", "small", "probe", "serve"])
+    ap.add_argument("--serve-jobs", type=int, default=120)
+    ap.add_argument("--serve-rates", default="10,100,500,2000")
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--probe-n", type=int, default=1 << 28,
                     help="probe workload: positions per step (split over the materials)")
     ap.add_argument("--probe-materials", default="KRRRvKRR,KQRvKRR",
@@ -804,6 +813,114 @@ def run_probe_reference(a, rank, world, local):
     }
 
 
+# ------------------------------------------------------------ serving loop
+SERVE_METRIC = "serving positions/s (continuous batching), p50/p99 latency"
+SERVE_PLY = ("KRRRvKRRR", "KQRvKRRR", "KQRRvKRR")
+
+
+def run_serve(a, rank, world, local):
+    """A seeded Poisson stream (seed 4) of 70% single-slice ply jobs on the
+    mix materials and 30% probe batches of 1k-1M positions on the probe
+    tables, served with continuous batching under an HBM admission budget
+    (pinned-host spill), at each rate of the sweep; beside it the same
+    stream served one request at a time (plain serial launches)."""
+    import torch
+
+    import tb8gen_b200 as tbg
+    from tb8gen_b200.serve import GpuExecutor, Scheduler, make_requests, summarize
+
+    torch.cuda.set_device(local)
+    tbg.init()
+    tbg.set_stub(1)
+    pool_n = 1 << 20
+    tables, pools = {}, {}
+    for m in PROBE_MATS:
+        tables[m] = tbg.DeviceTable(m, PROBE_SEED, 3)
+        q = torch.empty(pool_n * 16, dtype=torch.uint8, device="cuda")
+        tbg.gen_positions(m, 4, q)
+        pools[m] = q.cpu().pin_memory()
+        del q
+    ex = GpuExecutor(SERVE_PLY, tables, pools, slots=a.serve_slots,
+                     budget_bytes=int(a.serve_budget_gb * 1e9), probe_max=1_000_000)
+    rates = [float(r) for r in a.serve_rates.split(",")]
+    base = make_requests(a.serve_jobs, 1.0, SERVE_PLY, PROBE_MATS, seed=4, pool_n=pool_n)
+
+    def at_rate(rate):
+        return [type(r)(**{**r.__dict__, "arrival": r.arrival / rate}) for r in base]
+
+    # warm-up: every table bitmap the stream touches is built once, probe
+    # scratch grows to its largest batch
+    for m, t in tables.items():
+        q = torch.empty(1_000_000 * 16, dtype=torch.uint8, device="cuda")
+        q.copy_(pools[m][:1_000_000 * 16])
+        o = torch.empty(1_000_000, dtype=torch.int8, device="cuda")
+        tbg.set_stream(torch.cuda.current_stream())
+        t.probe(q, o, 0)
+        del q, o
+    torch.cuda.synchronize()
+    t0 = time.time()
+    Scheduler(ex, a.serve_slots).run(at_rate(1e9))
+    torch.cuda.synchronize()
+    warm_s = time.time() - t0
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
+    n0 = tbg.launches()
+    sweep = []
+    for rate in rates:
+        reqs = at_rate(rate)
+        recs, mk = Scheduler(ex, a.serve_slots).run(reqs)
+        cb = summarize(recs, mk)
+        recs1, mk1 = Scheduler(ex, 1).run(reqs)
+        se = summarize(recs1, mk1)
+        sweep.append({"rate_per_s": rate, "continuous": cb, "serial": se,
+                      "speedup": round(cb["positions_per_s"] / se["positions_per_s"], 3)})
+    launches = tbg.launches() - n0
+    clk = clocks.stop()
+    top = sweep[-1]
+    ply = [r for r in base if r.kind == "ply"]
+    prb = [r for r in base if r.kind == "probe"]
+    ply_pos = sum(ex.mpools[r.material].m.size for r in ply)
+    h2d = sum(r.n * 16 for r in prb)
+    d2h = sum(2 * ex.mpools[r.material].m.bytes for r in ply) + sum(r.n for r in prb)
+    value = top["continuous"]["positions_per_s"]
+    peak, peak_kind = measured_peak()
+    alg = ALG_BYTES_PER_POS * ply_pos
+    achieved = alg / top["continuous"]["makespan_s"] / 1e9
+    line = {
+        "metric": SERVE_METRIC, "value": value, "unit": "positions/s", "n_gpus": world,
+        "steps": len(rates), "warmup": 1,
+        "ms_per_step": round(1e3 * top["continuous"]["makespan_s"], 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64",
+        "data": "synthetic (seeded Poisson request stream, seeded inputs and tables)",
+        "config": {"workload": "serve", "jobs": len(base), "ply_jobs": len(ply),
+                   "probe_jobs": len(prb), "ply_materials": list(SERVE_PLY),
+                   "probe_materials": list(PROBE_MATS), "slots": a.serve_slots,
+                   "budget_gb": a.serve_budget_gb, "rates_per_s": rates, "seed": 4,
+                   "l2": "inputs larger than L2 (slice bitmaps and tables of GBs)"},
+        "sweep": sweep,
+        "p50_ms": top["continuous"]["p50_ms"], "p99_ms": top["continuous"]["p99_ms"],
+        "serial_positions_per_s": top["serial"]["positions_per_s"],
+        "memory": {"peak_gb": round(ex.peak / 1e9, 2), "spills": ex.spills,
+                   "reloads": ex.reloads, "builds": ex.builds},
+        "warmup_s": round(warm_s, 2),
+        "roofline": {"bound": "hbm", "kernel": "ply and probe mix",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 5), "peak_source": peak_kind,
+                     "traffic": None,
+                     "note": "ply algorithmic bytes (0.875 B/position) over the top-rate makespan"},
+        "gpu_launches": launches, "clocks": clk,
+        "e2e": {"value": value, "unit": "positions/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "note": "every request moves its payload and result through pinned host memory"},
+        "cpu_baseline": None,
+    }
+    for t in tables.values():
+        t.close()
+    return line
+
+
 def main():
     a = parse()
     rank, world, local = dist_env()
@@ -815,7 +932,13 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        if a.workload == "probe":
+        if a.workload == "serve":
+            line = None if a.impl == "reference" else run_serve(a, rank, world, local)
+            if a.impl == "reference" and rank == 0:
+                line = {"impl": "reference",
+                        "unavailable": "the reference has no serving loop; its per-job CPU "
+                                       "costs are the slice and probe reference arms"}
+        elif a.workload == "probe":
             line = (run_probe_reference if a.impl == "reference" else run_probe)(a, rank, world,
                                                                                   local)
         elif a.impl == "reference":

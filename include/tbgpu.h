@@ -277,7 +277,12 @@ int tbg_probe_close(int handle);
  * mode 0: queries grouped by rANS block, each touched block decoded once
  * (falls back to mode 1 for tables whose symbols cover unequal position
  * counts); mode 1: each query decoded on its own, as decompress_rans
- * (probe.c:1346-1390) does.  Both give identical results. */
+ * (probe.c:1346-1390) does.  Both give identical results.  Work is queued
+ * on the library's stream; the call returns without waiting when the
+ * scratch budget (tbg_probe_tune) holds min(n, table blocks) blocks, else it
+ * waits once to plan decode waves.  A handle's scratch serves every batch
+ * on it: batches on one handle must not overlap on the GPU (keep them on one
+ * stream, or open one handle per concurrent stream). */
 int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t n, void *dev_out, int mode);
 
 /* Where side `side` of an open table keeps its rANS blocks: byte offset of

@@ -365,10 +365,16 @@ __device__ __forceinline__ int dec_get_packed(uint64_t &x, const uint64_t *tab) 
 // at most one word).
 template <typename TS>
 __global__ void __launch_bounds__(256) k_probe_decode(ProbeSide S, const uint32_t *list,
-                                                      uint32_t t0, uint32_t t1, uint32_t wbase,
-                                                      uint32_t W, const uint32_t *minlit,
-                                                      TS *scratch) {
+                                                      uint32_t t0, uint32_t t1,
+                                                      const uint32_t *bounds, int bside,
+                                                      uint32_t wbase, uint32_t W,
+                                                      const uint32_t *minlit, TS *scratch) {
   __shared__ uint64_t tab[4096];
+  if (bounds) {  // touched range of this side, from k_probe_bounds
+    t0 = bside ? bounds[1] : 0u;
+    t1 = bside ? bounds[0] : bounds[1];
+    if (t0 >= t1) return;
+  }
   for (int b = threadIdx.x; b < 4096; b += blockDim.x) tab[b] = pack_bucket(S, b);
   __syncthreads();
   for (uint32_t t = t0 + blockIdx.x * blockDim.x + threadIdx.x; t < t1;
@@ -417,6 +423,18 @@ __global__ void __launch_bounds__(256) k_probe_decode(ProbeSide S, const uint32_
         }
       }
     }
+  }
+}
+
+// Device-side extent of a batch's touched blocks: bounds[0] = touched
+// blocks, bounds[1] = touched blocks of side 0 (tpos at side 1's first key;
+// key1 == nkeys for a one-sided table).
+__global__ void k_probe_bounds(const uint32_t *count, const uint32_t *tpos, uint64_t nkeys,
+                               uint64_t key1, uint32_t *bounds) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint32_t total = tpos[nkeys - 1] + (count[nkeys - 1] ? 1u : 0u);
+    bounds[0] = total;
+    bounds[1] = key1 < nkeys ? tpos[key1] : total;
   }
 }
 

@@ -316,6 +316,8 @@ struct ProbeHandle {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   bool timed = false;
   uint64_t touched = 0;        // blocks decoded by the last grouped batch
+  bool touched_on_device = false;  // ... still in bounds[0] (no host read yet)
+  uint32_t *bounds = nullptr;  // touched blocks, touched blocks of side 0
 };
 
 static ProbeHandle g_probe[8];
@@ -489,8 +491,8 @@ static int decode_waves(ProbeHandle &H, uint64_t n, int L, uint32_t ntouched, ui
       const uint32_t t0 = std::max(w0, b ? nside0 : 0u), t1 = std::min(w1, b ? ntouched : nside0);
       if (t0 >= t1) continue;
       const uint32_t grid_d = std::min<uint32_t>((t1 - t0 + 255) / 256, g_eng.num_sms * 7);
-      k_probe_decode<TS><<<grid_d, 256, 0, st>>>(H.P.side[b], H.list, t0, t1, w0, W, H.minlit,
-                                                 scratch);
+      k_probe_decode<TS><<<grid_d, 256, 0, st>>>(H.P.side[b], H.list, t0, t1, nullptr, b, w0, W,
+                                                 H.minlit, scratch);
     }
     if (w1 == ntouched) PCK(cudaEventRecord(H.ev[2], st));
     k_probe_answer<TS><<<grid, 256, 0, st>>>(H.P, H.key, H.lit, H.tpos, n, w0, W, scratch, out);
@@ -498,6 +500,31 @@ static int decode_waves(ProbeHandle &H, uint64_t n, int L, uint32_t ntouched, ui
     if (rc) return rc;
   }
   return TBG_OK;
+}
+
+// One wave of W = min(n, blocks) columns; the touched extent stays on the
+// device (k_probe_bounds), so the call does not wait for the GPU.
+template <typename TS>
+static int decode_async(ProbeHandle &H, uint64_t n, uint32_t W, int8_t *out) {
+  cudaStream_t st = g_eng.stream;
+  const bool two = H.P.side[1].nblocks != 0;
+  const int L = std::min(H.P.side[0].sym_positions, two ? H.P.side[1].sym_positions : 1 << 20);
+  const uint64_t per_block = (uint64_t)((kBlockPositions + L - 1) / L) * sizeof(TS);
+  int rc = grow_buf(&H.symbuf, &H.cap_sym, (uint64_t)W * per_block);
+  if (rc) return rc;
+  TS *scratch = reinterpret_cast<TS *>(H.symbuf);
+  k_probe_bounds<<<1, 32, 0, st>>>(H.count, H.tpos, H.nkeys, two ? H.P.side[1].key0 : H.nkeys,
+                                   H.bounds);
+  PCK(cudaEventRecord(H.ev[1], st));
+  const uint32_t grid_d = std::min<uint32_t>((W + 255) / 256, g_eng.num_sms * 7);
+  for (int b = 0; b < (two ? 2 : 1); b++)
+    k_probe_decode<TS><<<grid_d, 256, 0, st>>>(H.P.side[b], H.list, 0, 0, H.bounds, b, 0, W,
+                                               H.minlit, scratch);
+  PCK(cudaEventRecord(H.ev[2], st));
+  k_probe_answer<TS><<<g_eng.num_sms * 8, 256, 0, st>>>(H.P, H.key, H.lit, H.tpos, n, 0, W,
+                                                        scratch, out);
+  H.touched_on_device = true;
+  return g_eng.check_launch("probe decode");
 }
 
 static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, int mode) {
@@ -526,6 +553,7 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
     PCK(cudaMalloc(&H.tpos, H.nkeys * sizeof(uint32_t)));
     PCK(cudaMalloc(&H.list, H.nkeys * sizeof(uint32_t)));
     PCK(cudaMalloc(&H.tile, 2 * ntiles * sizeof(uint32_t)));
+    PCK(cudaMalloc(&H.bounds, 2 * sizeof(uint32_t)));
   }
   PCK(cudaEventRecord(H.ev[0], st));
   PCK(cudaMemsetAsync(H.count, 0, H.nkeys * 4, st));
@@ -536,9 +564,25 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
   k_scan_finish<<<ntiles, 1024, 0, st>>>(H.count, H.nkeys, H.tile + ntiles, H.tpos, H.list);
   rc = g_eng.check_launch("probe grouping");
   if (rc) return rc;
-  // touched blocks (the last key's scan value) and the touched blocks of
-  // side 0 (tpos at side 1's first key)
   const bool two = H.P.side[1].nblocks != 0;
+  int L = H.P.side[0].sym_positions;
+  if (two) L = std::min(L, H.P.side[1].sym_positions);
+  const bool narrow = H.P.side[0].nsym_emit <= 256 && (!two || H.P.side[1].nsym_emit <= 256);
+  // A batch touches at most min(n, blocks) blocks: when the scratch budget
+  // holds that many, one wave sized so runs without the host reading the
+  // touched count (no synchronisation inside the call).
+  const uint64_t wmax = std::min<uint64_t>(n, H.nkeys);
+  const uint64_t per_block = (uint64_t)((kBlockPositions + L - 1) / L) * (narrow ? 1 : 2);
+  if (wmax * per_block <= g_probe_scratch) {
+    rc = narrow ? decode_async<uint8_t>(H, n, (uint32_t)wmax, out)
+                : decode_async<uint16_t>(H, n, (uint32_t)wmax, out);
+    if (rc) return rc;
+    PCK(cudaEventRecord(H.ev[3], st));
+    H.timed = true;
+    return TBG_OK;
+  }
+  // touched blocks (the last key's scan value) and the touched blocks of
+  // side 0 (tpos at side 1's first key), read by the host to plan the waves
   uint32_t last[3] = {0, 0, 0};
   PCK(cudaMemcpyAsync(&last[0], H.tpos + H.nkeys - 1, 4, cudaMemcpyDeviceToHost, st));
   PCK(cudaMemcpyAsync(&last[1], H.count + H.nkeys - 1, 4, cudaMemcpyDeviceToHost, st));
@@ -547,10 +591,8 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
   const uint32_t ntouched = last[0] + (last[1] ? 1 : 0);
   const uint32_t nside0 = two ? last[2] : ntouched;
   H.touched = ntouched;
+  H.touched_on_device = false;
   if (ntouched == 0) return TBG_OK;
-  int L = H.P.side[0].sym_positions;
-  if (two) L = std::min(L, H.P.side[1].sym_positions);
-  const bool narrow = H.P.side[0].nsym_emit <= 256 && (!two || H.P.side[1].nsym_emit <= 256);
   rc = narrow ? decode_waves<uint8_t>(H, n, L, ntouched, nside0, out)
               : decode_waves<uint16_t>(H, n, L, ntouched, nside0, out);
   if (rc) return rc;
@@ -590,7 +632,7 @@ extern "C" int tbg_probe_close(int handle) {
     if (e) cudaEventDestroy(e);
   for (void *p : {(void *)H.dev_alloc, (void *)H.key, (void *)H.lit, (void *)H.count,
                   (void *)H.minlit, (void *)H.tpos, (void *)H.list, (void *)H.tile,
-                  (void *)H.symbuf})
+                  (void *)H.bounds, (void *)H.symbuf})
     if (p) cudaFree(p);
   H = ProbeHandle();
   return TBG_OK;
@@ -673,6 +715,12 @@ extern "C" int tbg_probe_phase_ms(int handle, float ms[3], uint64_t *touched_blo
   PCK(cudaEventElapsedTime(&ms[0], H.ev[0], H.ev[1]));
   PCK(cudaEventElapsedTime(&ms[1], H.ev[1], H.ev[2]));
   PCK(cudaEventElapsedTime(&ms[2], H.ev[2], H.ev[3]));
+  if (H.touched_on_device) {
+    uint32_t t = 0;
+    PCK(cudaMemcpy(&t, H.bounds, sizeof t, cudaMemcpyDeviceToHost));
+    H.touched = t;
+    H.touched_on_device = false;
+  }
   if (touched_blocks) *touched_blocks = H.touched;
   return TBG_OK;
 }
