@@ -16,6 +16,9 @@ Workloads (synthetic, seeded; there is no public dataset for this path):
          batches (30%, 1k-1M positions) served with continuous batching under
          an HBM admission budget, swept over arrival rates, beside one
          request at a time; p50/p99 latency and positions/s.
+  fixpoint  the whole generation of a material (default KQRvKRR) by the
+         C host driver with the planes in host memory (tbgen -S); per
+         half-ply positions/s; the resident run must print the same counts.
   probe  2^28 seeded legal positions (seed 3), half KRRRvKRR, half KQRvKRR,
          probed (WDL) against the synthetic rANS tables of the two
          materials (seed 3, values mod 3); a step is one probe batch of all
@@ -55,7 +58,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="slice",
-                    choices=["slice", "mix", "small", "probe", "serve"])
+                    choices=["slice", "mix", "small", "probe", "serve", "fixpoint"])
+    ap.add_argument("--fix-material", default="KQRvKRR")
+    ap.add_argument("--fix-max-ply", type=int, default=0)
     ap.add_argument("--serve-jobs", type=int, default=120)
     ap.add_argument("--serve-rates", default="10,100,500,2000")
     ap.add_argument("--serve-slots", type=int, default=8)
@@ -421,7 +426,7 @@ def run_cpu_baseline(a, jobs, budget=None, inputs=None, oracle=None):
             "phase_s": {k: round(v, 4) for k, v in c.times.items()}}
 
 
-def run_reference(a, rank, world, local):
+def run_reference(a, rank, world, local, spec=None):
     """Reference arm: the reference's own CPU workers (oracle/_ref) on all
     host cores, inputs built on the CPU by the same workers (no engine)."""
     if rank != 0:
@@ -429,7 +434,7 @@ def run_reference(a, rank, world, local):
     from oracle.plyjob_cpu import inputs_from_oracle
 
     cores = os.cpu_count() or 1
-    mat, s, p, seed = workload_spec(a.workload)[0]
+    mat, s, p, seed = spec or workload_spec(a.workload)[0]
     O, kind = cpu_oracle(mat, cores)
     O.set_stub(1, 3)
     t0 = time.time()
@@ -921,6 +926,96 @@ def run_serve(a, rank, world, local):
     return line
 
 
+# ------------------------------------------------------------ fixpoint
+FIX_METRIC = "fixpoint ply positions/s (streamed, host tier)"
+
+
+def parse_tbgen(stderr):
+    times, stats = [], {}
+    for line in stderr.splitlines():
+        if line.startswith("time "):
+            f = line.split()
+            kind = f[1]
+            kv = dict(x.split("=") for x in f[2:])
+            times.append((kind, float(kv["ms"]), int(kv["positions"])))
+        elif line.startswith("stats "):
+            stats = {k: int(v) for k, v in (x.split("=") for x in line.split()[1:])}
+    return times, stats
+
+
+def run_fixpoint(a, rank, world, local):
+    """The whole generation of one material (calc_sub, illegal and mate,
+    then calc_L_n / calc_W_n until no bitmap changes) by the C host driver
+    in streamed mode: planes in host memory, a device window of slices.
+    The same generation in resident mode must print the same counts."""
+    import torch
+
+    from tb8gen_b200 import build
+
+    if rank != 0:
+        return None
+    tbgen = build.build_host()
+    mat = a.fix_material
+    base = [tbgen, "-s", "1", "-m", "3", "-p"]
+    if a.fix_max_ply:
+        base += ["-n", str(a.fix_max_ply)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
+    t0 = time.time()
+    r = subprocess.run(base + ["-S", mat], capture_output=True, text=True, timeout=3000)
+    wall = time.time() - t0
+    clk = clocks.stop()
+    if r.returncode != 0:
+        raise RuntimeError("tbgen failed: " + r.stderr[-2000:])
+    times, stats = parse_tbgen(r.stderr)
+    counts = [l.strip() for l in r.stdout.splitlines() if " = " in l]
+    r2 = subprocess.run(base + [mat], capture_output=True, text=True, timeout=3000)
+    counts2 = [l.strip() for l in r2.stdout.splitlines() if " = " in l]
+    t2, _ = parse_tbgen(r2.stderr)
+    ms = sum(t for _, t, _ in times)
+    pos = sum(p for _, _, p in times)
+    alg = sum((0.5 if k.startswith("w") else 0.375) * p for k, _, p in times)
+    value = pos / (ms / 1e3)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms / 1e3) / 1e9
+    cpu = None
+    if not a.no_cpu:
+        from oracle.plyjob_cpu import inputs_from_oracle
+
+        O, kind = cpu_oracle(mat, os.cpu_count() or 1)
+        O.set_stub(1, 3)
+        cpu = run_cpu_baseline(a, None, budget=min(a.cpu_seconds, 15.0),
+                               inputs=inputs_from_oracle(O, mat, 96, 0.01, 1), oracle=(O, kind))
+    plies = stats.get("plies", 0)
+    return {
+        "metric": FIX_METRIC, "value": round(value, 1), "unit": "positions/s", "n_gpus": world,
+        "steps": len(times), "warmup": 0, "ms_per_step": round(ms / max(len(times), 1), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded 7-piece stub; the generation itself is deterministic)",
+        "config": {"workload": "fixpoint", "material": mat, "mode": "streamed",
+                   "plies": plies, "half_plies": len(times),
+                   "note": "a step is one half-ply (calc_W_n or calc_L_n) over all 462 slices",
+                   "l2": "slice planes of the whole material stream through the device"},
+        "total_s": round(wall, 2), "half_ply_ms_total": round(ms, 1),
+        "resident_half_ply_ms_total": round(sum(t for _, t, _ in t2), 1),
+        "counts_match_resident": counts == counts2 and r2.returncode == 0,
+        "count_lines": len(counts), "last_counts": counts[-4:],
+        "roofline": {"bound": "hbm", "kernel": "half-ply (all kernels)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 5), "peak_source": peak_kind,
+                     "traffic": None,
+                     "note": "0.5 B (W) / 0.375 B (L) per position over the half-ply time; "
+                             "host-tier copies included"},
+        "gpu_launches": stats.get("launches"), "clocks": clk,
+        "e2e": {"value": round(value, 1), "unit": "positions/s",
+                "h2d_bytes_per_step": stats.get("h2d_bytes", 0) // max(len(times), 1),
+                "d2h_bytes_per_step": stats.get("d2h_bytes", 0) // max(len(times), 1),
+                "note": "streamed mode: every slice moves through host memory"},
+        "cpu_baseline": cpu,
+    }
+
+
 def main():
     a = parse()
     rank, world, local = dist_env()
@@ -932,7 +1027,18 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        if a.workload == "serve":
+        if a.workload == "fixpoint":
+            line = None
+            if a.impl == "reference":
+                # a whole generation by the reference takes hours on the host
+                # cores: its arm times the reference's slice-ply of the same
+                # material (slice 96, sources Bernoulli(0.01))
+                line = run_reference(a, rank, world, local, (a.fix_material, 96, 0.01, 1))
+                if line:
+                    line["metric"] = FIX_METRIC
+            else:
+                line = run_fixpoint(a, rank, world, local)
+        elif a.workload == "serve":
             line = None if a.impl == "reference" else run_serve(a, rank, world, local)
             if a.impl == "reference" and rank == 0:
                 line = {"impl": "reference",

@@ -106,6 +106,13 @@ int tbg_set_stub(uint64_t seed, int modulus);
 int tbg_alloc(size_t bytes, void **dev);
 int tbg_free(void *dev);
 
+/* Copies between host memory and device memory on the library's stream,
+ * returning when the copy is done: the host tier of a C host that keeps
+ * slices in host memory (in place of kslice_read / kslice_write,
+ * kslice.c:317-379). */
+int tbg_copy_to_device(void *dev, const void *host, size_t bytes);
+int tbg_copy_to_host(void *host, const void *dev, size_t bytes);
+
 /* ---- slot map (kslice_slot / kslice_buf / kslice_sub_buf) ------------ */
 
 /* Binds a device bitmap of `bytes` bytes to slice s of the current

@@ -965,6 +965,22 @@ extern "C" int tbg_free(void *dev) {
   return TBG_OK;
 }
 
+extern "C" int tbg_copy_to_device(void *dev, const void *host, size_t bytes) {
+  if (!dev || !host) return fail(TBG_ERR_ARG, "null pointer");
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, g_eng.stream));
+  CK(cudaStreamSynchronize(g_eng.stream));
+  return TBG_OK;
+}
+
+extern "C" int tbg_copy_to_host(void *host, const void *dev, size_t bytes) {
+  if (!dev || !host) return fail(TBG_ERR_ARG, "null pointer");
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, g_eng.stream));
+  CK(cudaStreamSynchronize(g_eng.stream));
+  return TBG_OK;
+}
+
 namespace tbg {
 __global__ void __launch_bounds__(kThreads) k_and_not3(uint4 *d, const uint4 *a, const uint4 *b,
                                                        uint64_t n16) {

@@ -3,24 +3,36 @@
  * calc_sub_kslices, calc_illegal_and_mate, calc_L_n, calc_W_n) as a C host
  * over the tbgpu C ABI, with every king slice resident in HBM.
  *
- *   tbgen [-s seed] [-m 3|5] [-q] MATERIAL
+ *   tbgen [-s seed] [-m 3|5] [-b device_MB] [-S] [-p] [-n max_ply] MATERIAL
  *
  * Prints the reference's per-ply counts ("broken_w = ...", "l<n>_<c> = ...",
- * "w<n>_<c> = ...") in the reference's order.  There is no disk tier: each
+ * "w<n>_<c> = ...") in the reference's order.
+ *
+ * Resident mode (default when everything fits the device budget -b): each
  * slice's "wins", the previous and current W/L bitmaps of both sides and the
  * capture-class bitmaps stay on the device for the whole run, so the
  * reference's KSliceManager window (kslice.c:41-84) reduces to "all slices
  * bound": the order in which slices are scattered does not change a bitmap
  * (marks are ORed), and every scatter of a half-ply finishes before its
- * epilogue or verify starts, as in the reference.  7-piece capture values
- * come from the seeded stub (tbg_set_stub); a capture that leaves the two
- * kings alone is a draw, as in the reference.
+ * epilogue or verify starts, as in the reference.
+ *
+ * Streamed mode (-S, or when the planes exceed -b): the planes live in host
+ * memory, the tier that replaces the reference's slice files
+ * (kslice_read/kslice_write, kslice.c:317-379), and the device holds a
+ * window of slices that follows the schedule's slice order, as the
+ * reference's manager does: a slice is brought in before the first step
+ * that unmoves into it (or reads it) and written out after the last one.
+ *
+ * -p prints a timing line per half-ply ("time <kind><n>_<c> ms=...").
+ * 7-piece capture values come from the seeded stub (tbg_set_stub); a capture
+ * that leaves the two kings alone is a draw, as in the reference.
  */
 #define _POSIX_C_SOURCE 200809L
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #include <unistd.h>
 
 #include "../../include/tbgpu.h"
@@ -161,78 +173,499 @@ static int calc_W_n(int stm, int n, int more_w)
   return cnt != 0;
 }
 
+
+/* ------------------------------------------------------------ streamed mode */
+static uint64_t g_size;        /* positions per slice */
+static int g_timing;
+
+static double now_ms(void)
+{
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+}
+
+/* The host tier's reads and writes (kslice_read / kslice_write,
+ * kslice.c:317-379), through the library's stream. */
+static uint64_t g_h2d_bytes, g_d2h_bytes;
+
+static void h2d(void *dev, const void *host, size_t n)
+{
+  ok(tbg_copy_to_device(dev, host, n), "copy to device");
+  g_h2d_bytes += n;
+}
+
+static void d2h(void *host, const void *dev, size_t n)
+{
+  ok(tbg_copy_to_host(host, dev, n), "copy to host");
+  g_d2h_bytes += n;
+}
+
+/* King-pair tables, generated from their rules (probe.c:441-539,
+ * tb8gen.c:69-89): KKIdx over the a1-d1-d4 triangle, KKSquare, KKMap. */
+static int KKIdx[10][64], KKSq[NS][2], KKMap[64][64];
+
+static uint64_t katt(int sq)
+{
+  uint64_t b = 0;
+  for (int df = -1; df <= 1; df++)
+    for (int dr = -1; dr <= 1; dr++) {
+      int f = (sq & 7) + df, r = (sq >> 3) + dr;
+      if ((df || dr) && f >= 0 && f < 8 && r >= 0 && r < 8) b |= 1ULL << (r * 8 + f);
+    }
+  return b;
+}
+
+static void init_king_tables(void)
+{
+  static const int tri[10] = { 1, 2, 3, 10, 11, 19, 0, 9, 18, 27 };
+  int next = 0, nd = 441;
+  for (int t = 0; t < 10; t++)
+    for (int sq = 0; sq < 64; sq++) {
+      KKIdx[t][sq] = -1;
+      if (sq == tri[t] || (katt(tri[t]) >> sq & 1)) continue;
+      if (t >= 6) {
+        if ((sq & 7) < (sq >> 3)) continue;
+        if ((sq & 7) == (sq >> 3)) {
+          KKIdx[t][sq] = nd++;
+          continue;
+        }
+      }
+      KKIdx[t][sq] = next++;
+    }
+  for (int t = 0; t < 10; t++)
+    for (int sq = 0; sq < 64; sq++)
+      if (KKIdx[t][sq] >= 0) {
+        KKSq[KKIdx[t][sq]][0] = tri[t];
+        KKSq[KKIdx[t][sq]][1] = sq;
+      }
+  int triangle[64];
+  for (int sq = 0; sq < 64; sq++) {
+    int f = sq & 7, r = sq >> 3;
+    if (f > 3) f = 7 - f;
+    if (r > 3) r = 7 - r;
+    if (r > f) { int x = f; f = r; r = x; }
+    for (int t = 0; t < 10; t++)
+      if (tri[t] == r * 8 + f) triangle[sq] = t;
+  }
+  for (int i = 0; i < 64; i++)
+    for (int j = 0; j < 64; j++) {
+      int m = ((i & 7) >= 4 ? 0x07 : 0) | ((i >> 3) >= 4 ? 0x38 : 0);
+      int s1 = i ^ m, s2 = j ^ m;
+      int tri_ok = (s1 & 7) <= 3 && (s1 >> 3) <= (s1 & 7);
+      int diag = tri_ok && (s1 & 7) == (s1 >> 3);
+      int lower = (s2 & 7) >= (s2 >> 3);
+      if (!tri_ok || (diag && !lower)) {
+        s1 = ((s1 & 7) << 3) | (s1 >> 3);
+        s2 = ((s2 & 7) << 3) | (s2 >> 3);
+      }
+      KKMap[i][j] = (i == j || (katt(i) >> j & 1)) ? -1 : KKIdx[triangle[s1]][s2];
+    }
+}
+
+/* The slices a step on slice s of side stm touches: s and the slices its
+ * king moves reach (the targets of predecessors, the wins that
+ * check_successors reads). */
+static int step_slices(int stm, int s, int *out)
+{
+  int n = 0, me = KKSq[s][stm], opp = KKSq[s][stm ^ 1];
+  out[n++] = s;
+  uint64_t b = katt(me) & ~katt(opp) & ~(1ULL << opp);
+  while (b) {
+    int to = __builtin_ctzll(b);
+    b &= b - 1;
+    int k[2] = { KKSq[s][0], KKSq[s][1] };
+    k[stm] = to;
+    int t = KKMap[k[0]][k[1]];
+    int seen = t < 0;
+    for (int j = 0; j < n && !seen; j++) seen = out[j] == t;
+    if (!seen) out[n++] = t;
+  }
+  return n;
+}
+
+/* Step order per side to move: for black, the rows of KKIdx (black-king
+ * moves keep the normalised white king, so they stay within a row); for
+ * white, the same steps through the colour flip, as the reference's
+ * manager (kslice.c:41-84) orders them. */
+static int order[2][NS];
+static int touch[2][NS][12], ntouch[2][NS];
+static int last_use[2][NS];
+static int window_max;
+
+static void init_schedule(void)
+{
+  int k = 0;
+  for (int i = 0; i < 10; i++)
+    for (int bk = 0; bk < 64; bk++)
+      if (KKIdx[i][bk] >= 0) order[BLACK][k++] = KKIdx[i][bk];
+  for (k = 0; k < NS; k++) {
+    int s = order[BLACK][k];
+    order[WHITE][k] = KKMap[KKSq[s][1]][KKSq[s][0]];
+  }
+  for (int stm = 0; stm < 2; stm++) {
+    int live = 0, resident[NS] = { 0 };
+    for (k = 0; k < NS; k++) {
+      ntouch[stm][k] = step_slices(stm, order[stm][k], touch[stm][k]);
+      for (int j = 0; j < ntouch[stm][k]; j++) last_use[stm][touch[stm][k][j]] = k;
+    }
+    for (k = 0; k < NS; k++) {
+      for (int j = 0; j < ntouch[stm][k]; j++)
+        if (!resident[touch[stm][k][j]]) {
+          resident[touch[stm][k][j]] = 1;
+          live++;
+        }
+      if (live > window_max) window_max = live;
+      for (int j = 0; j < ntouch[stm][k]; j++) {
+        int t = touch[stm][k][j];
+        if (last_use[stm][t] == k && resident[t]) {
+          resident[t] = 0;
+          live--;
+        }
+      }
+    }
+  }
+}
+
+/* host tier: per side the planes of all slices */
+enum { P_WINS, P_WP, P_LP, P_WC, P_LC, P_X, NPLANE };
+static uint8_t *HP[2][NPLANE], *HS[2][5];
+#define HSL(plane, c, s) (HP[c][plane] + (size_t)(s) * g_bytes)
+#define HSUB(c, k, s) (HS[c][k] + (size_t)(s) * g_sub)
+
+/* device window */
+static uint8_t **wbuf, **wsub, *dsrc, *dwins, *dsub_src, *dsub_tmp;
+static int *wfree, nfree, where_[NS];
+
+static int take(void)
+{
+  if (nfree == 0) {
+    fprintf(stderr, "tbgen: window exhausted\n");
+    exit(EXIT_FAILURE);
+  }
+  return wfree[--nfree];
+}
+
+static void give(int b) { wfree[nfree++] = b; }
+
+static void st_calc_subs(void)
+{
+  for (int stm = 0; stm < 2; stm++)
+    for (int s = 0; s < NS; s++) {
+      void *cls[5] = { wsub[0], wsub[1], wsub[2], wsub[3], wsub[4] };
+      ok(tbg_calc_sub(stm, s, cls), "calc_sub");
+      for (int k = 0; k < 5; k++) d2h(HSUB(stm, k, s), wsub[k], g_sub);
+    }
+}
+
+static void st_illegal_and_mate(void)
+{
+  uint64_t cnt[4] = { 0, 0, 0, 0 }, c;
+  for (int s = 0; s < NS; s++) {
+    uint8_t *b[4] = { wbuf[0], wbuf[1], wbuf[2], wbuf[3] };
+    ok(tbg_calc_illegal(s, b[0], b[1]), "illegal");
+    ok(tbg_calc_mate(s, b[0], b[1], b[2], b[3]), "mate");
+    for (int j = 0; j < 4; j++) {
+      ok(tbg_slot_bind(0, b[j], g_bytes), "bind");
+      ok(tbg_count(0, &c), "count");
+      cnt[j] += c;
+    }
+    ok(tbg_slot_bind(0, NULL, 0), "unbind");
+    d2h(HSL(P_WINS, WHITE, s), b[0], g_bytes);
+    d2h(HSL(P_WINS, BLACK, s), b[1], g_bytes);
+    d2h(HSL(P_LP, WHITE, s), b[2], g_bytes);
+    d2h(HSL(P_LP, BLACK, s), b[3], g_bytes);
+  }
+  printf("broken_w = %llu\nbroken_b = %llu\nl0_w = %llu\nl0_b = %llu\n",
+         (unsigned long long)cnt[0], (unsigned long long)cnt[1], (unsigned long long)cnt[2],
+         (unsigned long long)cnt[3]);
+}
+
+/* Brings slice t into the window for a scatter (cleared target). */
+static void enter_target(int t)
+{
+  if (where_[t] >= 0) return;
+  int b = take();
+  where_[t] = b;
+  ok(tbg_slot_bind(t, wbuf[b], g_bytes), "bind");
+  ok(tbg_clear(t), "clear");
+}
+
+static void leave(int t)
+{
+  ok(tbg_slot_bind(t, NULL, 0), "unbind");
+  ok(tbg_sub_bind(t, NULL, 0), "unbind sub");
+  give(where_[t]);
+  where_[t] = -1;
+}
+
+/* calc_W_n streamed (tb8gen.c:1028-1084). */
+static int st_calc_W_n(int stm, int n, int more_w)
+{
+  uint64_t cnt = 0, c;
+  for (int k = 0; k < NS; k++) {
+    int s = order[stm][k];
+    for (int j = 0; j < ntouch[stm][k]; j++) enter_target(touch[stm][k][j]);
+    if (n == 1 || n == DRAW_RULE + 1) {
+      h2d(dsub_src, HSUB(stm ^ 1, n == 1 ? C_LOSS : C_BLOSS, s), g_sub);
+      ok(tbg_sub_bind(s, dsub_src, g_sub), "bind sub");
+      ok(tbg_predecessors_sub(stm, s, 0), "predecessors_sub");
+      ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
+    }
+    if (more_w) {
+      h2d(dsrc, HSL(P_LP, stm ^ 1, s), g_bytes);
+      ok(tbg_slot_bind(-1, dsrc, g_bytes), "bind");
+      ok(tbg_predecessors(stm, s), "predecessors");
+    }
+    for (int j = 0; j < ntouch[stm][k]; j++) {
+      int t = touch[stm][k][j];
+      if (last_use[stm][t] != k) continue;
+      h2d(dwins, HSL(P_WINS, stm, t), g_bytes);
+      ok(tbg_epilogue_W_to(t, dwins, dwins, &c), "epilogue");
+      cnt += c;
+      d2h(HSL(P_WC, stm, t), wbuf[where_[t]], g_bytes);
+      d2h(HSL(P_WINS, stm, t), dwins, g_bytes);
+      leave(t);
+    }
+  }
+  printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
+  return cnt != 0;
+}
+
+/* calc_L_n streamed (tb8gen.c:943-1026): candidates, written to the X
+ * plane, then the verify. */
+static int st_calc_L_n(int stm, int n, int more_l)
+{
+  uint64_t cnt = 0, c;
+  for (int k = 0; k < NS; k++) {
+    int s = order[stm][k];
+    for (int j = 0; j < ntouch[stm][k]; j++) enter_target(touch[stm][k][j]);
+    if (n == 1) {
+      h2d(dsub_src, HSUB(stm ^ 1, C_WIN, s), g_sub);
+      ok(tbg_sub_bind(s, dsub_src, g_sub), "bind sub");
+      ok(tbg_predecessors_sub(stm, s, 1), "predecessors_sub");
+      ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
+    } else if (n == DRAW_RULE + 1) {
+      /* cwin \ win (tb8gen.c:964-970) */
+      h2d(dsub_src, HSUB(stm ^ 1, C_CWIN, s), g_sub);
+      h2d(dsub_tmp, HSUB(stm ^ 1, C_WIN, s), g_sub);
+      ok(tbg_bitmap_and_not(dsub_src, dsub_src, dsub_tmp, g_sub), "and_not");
+      ok(tbg_sub_bind(s, dsub_src, g_sub), "bind sub");
+      ok(tbg_predecessors_sub(stm, s, 0), "predecessors_sub");
+      ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
+    }
+    if (more_l && n > 1) {
+      h2d(dsrc, HSL(P_WP, stm ^ 1, s), g_bytes);
+      ok(tbg_slot_bind(-1, dsrc, g_bytes), "bind");
+      ok(tbg_predecessors(stm, s), "predecessors");
+    }
+    for (int j = 0; j < ntouch[stm][k]; j++) {
+      int t = touch[stm][k][j];
+      if (last_use[stm][t] != k) continue;
+      d2h(HSL(P_X, stm, t), wbuf[where_[t]], g_bytes);
+      leave(t);
+    }
+  }
+  int cls = n <= DRAW_RULE ? C_WIN : C_CWIN;
+  for (int k = 0; k < NS; k++) {
+    int s = order[stm][k];
+    for (int j = 0; j < ntouch[stm][k]; j++) {
+      int t = touch[stm][k][j];
+      if (where_[t] >= 0) continue;
+      int b = take();
+      where_[t] = b;
+      h2d(wbuf[b], HSL(P_WINS, stm ^ 1, t), g_bytes);
+      h2d(wsub[b], HSUB(stm ^ 1, cls, t), g_sub);
+      ok(tbg_slot_bind(t, wbuf[b], g_bytes), "bind");
+      ok(tbg_sub_bind(t, wsub[b], g_sub), "bind sub");
+    }
+    h2d(dsrc, HSL(P_X, stm, s), g_bytes);
+    ok(tbg_slot_bind(-1, dsrc, g_bytes), "bind");
+    ok(tbg_check_successors(stm, s), "check_successors");
+    ok(tbg_count(-1, &c), "count");
+    cnt += c;
+    d2h(HSL(P_LC, stm, s), dsrc, g_bytes);
+    for (int j = 0; j < ntouch[stm][k]; j++) {
+      int t = touch[stm][k][j];
+      if (last_use[stm][t] == k) leave(t);
+    }
+  }
+  printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
+  return cnt != 0;
+}
+
+static void *host_alloc(size_t n)
+{
+  void *p = malloc(n);
+  if (!p) {
+    fprintf(stderr, "tbgen: out of host memory (%zu bytes)\n", n);
+    exit(EXIT_FAILURE);
+  }
+  return p;
+}
+
+/* Sets up the streamed mode: host planes and the device window. */
+static void st_setup(void)
+{
+  init_king_tables();
+  init_schedule();
+  int nbuf = window_max > 5 ? window_max : 5;
+  for (int c = 0; c < 2; c++) {
+    for (int p = 0; p < NPLANE; p++) HP[c][p] = host_alloc((size_t)g_bytes * NS);
+    for (int k = 0; k < 5; k++) HS[c][k] = host_alloc((size_t)g_sub * NS);
+  }
+  size_t total = (size_t)g_bytes * (nbuf + 2) + (size_t)g_sub * (nbuf + 2);
+  uint8_t *base;
+  ok(tbg_alloc(total, (void **)&base), "alloc");
+  wbuf = calloc(nbuf, sizeof *wbuf);
+  wsub = calloc(nbuf, sizeof *wsub);
+  wfree = calloc(nbuf, sizeof *wfree);
+  for (int b = 0; b < nbuf; b++) {
+    wbuf[b] = base;
+    base += g_bytes;
+    wsub[b] = base;
+    base += g_sub;
+    wfree[nfree++] = nbuf - 1 - b;
+  }
+  dsrc = base;
+  base += g_bytes;
+  dwins = base;
+  base += g_bytes;
+  dsub_src = base;
+  base += g_sub;
+  dsub_tmp = base;
+  for (int s = 0; s < NS; s++) where_[s] = -1;
+  if (!quiet)
+    fprintf(stderr, "tbgen: streamed, window of %d slices, host tier %.1f GB\n", nbuf,
+            (double)(NPLANE * g_bytes + 5 * g_sub) * NS * 2 / 1e9);
+}
+
+static void swap_host_planes(void)
+{
+  for (int c = 0; c < 2; c++) {
+    uint8_t *t = HP[c][P_WP];
+    HP[c][P_WP] = HP[c][P_WC];
+    HP[c][P_WC] = t;
+    t = HP[c][P_LP];
+    HP[c][P_LP] = HP[c][P_LC];
+    HP[c][P_LC] = t;
+  }
+}
+
+typedef int (*step_fn)(int stm, int n, int more);
+
+/* One half-ply call with its timing line (-p). */
+static int timed(step_fn f, const char *kind, int stm, int n, int more)
+{
+  double t0 = now_ms();
+  int r = f(stm, n, more);
+  if (g_timing) {
+    ok(tbg_sync(0), "sync");
+    double ms = now_ms() - t0;
+    fprintf(stderr, "time %s%d_%c ms=%.3f positions=%llu\n", kind, n, "wb"[stm], ms,
+            (unsigned long long)(g_size * NS));
+  }
+  return r;
+}
+
 int main(int argc, char **argv)
 {
   uint64_t seed = 1;
-  int mod = 3, opt;
-  while ((opt = getopt(argc, argv, "s:m:q")) != -1) {
+  int mod = 3, opt, force_stream = 0, max_ply = 1 << 30;
+  double budget_mb = 0;
+  while ((opt = getopt(argc, argv, "s:m:qb:Spn:")) != -1) {
     if (opt == 's') seed = strtoull(optarg, NULL, 10);
     else if (opt == 'm') mod = atoi(optarg);
     else if (opt == 'q') quiet = 1;
+    else if (opt == 'b') budget_mb = atof(optarg);
+    else if (opt == 'S') force_stream = 1;
+    else if (opt == 'p') g_timing = 1;
+    else if (opt == 'n') max_ply = atoi(optarg);
   }
   if (optind >= argc) {
-    fprintf(stderr, "usage: tbgen [-s seed] [-m 3|5] MATERIAL\n");
+    fprintf(stderr,
+            "usage: tbgen [-s seed] [-m 3|5] [-b device_MB] [-S] [-p] [-n max_ply] MATERIAL\n");
     return EXIT_FAILURE;
   }
   ok(tbg_init(), "init");
   ok(tbg_material_from_name(argv[optind]), "material");
   ok(tbg_set_stub(seed, mod), "stub");
-  uint64_t size, offs[6], capt[6];
-  ok(tbg_geometry(&size, &g_bytes, &g_sub, offs, capt), "geometry");
+  uint64_t offs[6], capt[6];
+  ok(tbg_geometry(&g_size, &g_bytes, &g_sub, offs, capt), "geometry");
 
-  /* one allocation for everything: 10 bitmap planes, 10 sub planes + temp */
+  /* resident: 10 bitmap planes, 10 sub planes + temp */
   size_t per = (size_t)g_bytes, persub = (size_t)g_sub;
   size_t total = per * NS * 10 + persub * NS * 11;
-  uint8_t *base;
-  ok(tbg_alloc(total, (void **)&base), "alloc");
-  uint8_t *p = base;
-  for (int c = 0; c < 2; c++)
-    for (int s = 0; s < NS; s++) {
-      wins[c][s] = p; p += per;
-      Wp[c][s] = p; p += per;
-      Lp[c][s] = p; p += per;
-      Wc[c][s] = p; p += per;
-      Lc[c][s] = p; p += per;
-    }
-  for (int c = 0; c < 2; c++)
-    for (int k = 0; k < 5; k++)
+  int streamed = force_stream || (budget_mb > 0 && total > budget_mb * 1e6);
+  step_fn W = calc_W_n, L = calc_L_n;
+  uint8_t *base = NULL;
+  if (streamed) {
+    st_setup();
+    st_calc_subs();
+    st_illegal_and_mate();
+    W = st_calc_W_n;
+    L = st_calc_L_n;
+  } else {
+    ok(tbg_alloc(total, (void **)&base), "alloc");
+    uint8_t *p = base;
+    for (int c = 0; c < 2; c++)
       for (int s = 0; s < NS; s++) {
-        sub[c][k][s] = p;
-        p += persub;
+        wins[c][s] = p; p += per;
+        Wp[c][s] = p; p += per;
+        Lp[c][s] = p; p += per;
+        Wc[c][s] = p; p += per;
+        Lc[c][s] = p; p += per;
       }
-  for (int s = 0; s < NS; s++) {
-    subtmp[s] = p;
-    p += persub;
+    for (int c = 0; c < 2; c++)
+      for (int k = 0; k < 5; k++)
+        for (int s = 0; s < NS; s++) {
+          sub[c][k][s] = p;
+          p += persub;
+        }
+    for (int s = 0; s < NS; s++) {
+      subtmp[s] = p;
+      p += persub;
+    }
+    calc_subs();
+    illegal_and_mate();  /* L0 into Lp */
   }
-
-  calc_subs();
-  illegal_and_mate();  /* L0 into Lp */
 
   int more_ww = 1, more_wb = 1, more_lw = 1, more_lb = 1, more_wb_next, more_ww_next;
   int n;
   /* tb8gen.c:1414-1444; after each ply the current W/L become the sources */
-  for (n = 1; ; n++) {
+  for (n = 1; n <= max_ply; n++) {
     int special = n == DRAW_RULE + 1;
     if (n > DRAW_RULE + 1 && !(more_ww || more_wb || more_lw || more_lb)) break;
     if (special) {
-      more_wb_next = calc_L_n(WHITE, n, more_lw);
-      more_ww_next = calc_L_n(BLACK, n, more_lb);
-      more_lb = calc_W_n(WHITE, n, more_ww);
-      more_lw = calc_W_n(BLACK, n, more_wb);
+      more_wb_next = timed(L, "l", WHITE, n, more_lw);
+      more_ww_next = timed(L, "l", BLACK, n, more_lb);
+      more_lb = timed(W, "w", WHITE, n, more_ww);
+      more_lw = timed(W, "w", BLACK, n, more_wb);
     } else {
-      more_wb_next = more_lw && calc_L_n(WHITE, n, more_lw);
-      more_ww_next = more_lb && calc_L_n(BLACK, n, more_lb);
-      more_lb = more_ww && calc_W_n(WHITE, n, more_ww);
-      more_lw = more_wb && calc_W_n(BLACK, n, more_wb);
+      more_wb_next = more_lw && timed(L, "l", WHITE, n, more_lw);
+      more_ww_next = more_lb && timed(L, "l", BLACK, n, more_lb);
+      more_lb = more_ww && timed(W, "w", WHITE, n, more_ww);
+      more_lw = more_wb && timed(W, "w", BLACK, n, more_wb);
     }
     more_wb = more_wb_next;
     more_ww = more_ww_next;
-    for (int c = 0; c < 2; c++) {
-      swap_planes(Wp[c], Wc[c]);
-      swap_planes(Lp[c], Lc[c]);
+    if (streamed) {
+      swap_host_planes();
+    } else {
+      for (int c = 0; c < 2; c++) {
+        swap_planes(Wp[c], Wc[c]);
+        swap_planes(Lp[c], Lc[c]);
+      }
     }
   }
   ok(tbg_sync(0), "sync");
-  ok(tbg_free(base), "free");
+  if (g_timing) {
+    uint64_t launches = 0;
+    ok(tbg_launches(&launches), "launches");
+    fprintf(stderr, "stats launches=%llu h2d_bytes=%llu d2h_bytes=%llu plies=%d\n",
+            (unsigned long long)launches, (unsigned long long)g_h2d_bytes,
+            (unsigned long long)g_d2h_bytes, n - 1);
+  }
+  if (base) ok(tbg_free(base), "free");
   return 0;
 }

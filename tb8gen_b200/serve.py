@@ -316,12 +316,16 @@ class GpuExecutor:
         stream = self.streams[slot]
         tbg.set_stream(stream)
         job = _Job(req, torch.cuda.Event())
-        with torch.cuda.stream(stream):
-            if req.kind == "ply":
-                self._issue_ply(job, stream)
-            else:
-                self._issue_probe(job, stream)
-            job.event.record(stream)
+        try:
+            with torch.cuda.stream(stream):
+                if req.kind == "ply":
+                    self._issue_ply(job, stream)
+                else:
+                    self._issue_probe(job, stream)
+                job.event.record(stream)
+        finally:
+            # later library calls of the caller go to its own current stream
+            tbg.set_stream(torch.cuda.current_stream())
         self.peak = max(self.peak, self.used)
         return job
 

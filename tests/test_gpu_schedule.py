@@ -36,3 +36,24 @@ def test_generation_counts_match_reference(material):
     assert r.returncode == 0, r.stderr
     got = [l.strip() for l in r.stdout.splitlines() if " = " in l]
     assert got == case["lines"]
+
+
+STREAMED = ["KRvK", "KRRvK", "KRvKN", "KRRvKR"]
+
+
+@pytest.mark.parametrize("material", STREAMED)
+def test_streamed_generation_counts_match_reference(material):
+    """The same generations with the planes in host memory and a device
+    window of slices that follows the schedule (tbgen -S): identical counts."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    case = CASES[material]
+    cmd = [TBGEN, "-S"]
+    if case["seed"] is not None:
+        cmd += ["-s", str(case["seed"]), "-m", str(case["mod"])]
+    r = subprocess.run(cmd + [material], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr
+    assert "streamed" in r.stderr
+    got = [l.strip() for l in r.stdout.splitlines() if " = " in l]
+    assert got == case["lines"]
