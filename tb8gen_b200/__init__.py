@@ -78,6 +78,7 @@ def lib():
             "tbg_probe_open": [vp, u64, C.c_char_p, C.POINTER(i)],
             "tbg_probe_close": [i],
             "tbg_probe_tune": [u64],
+            "tbg_tune_split": [i],
             "tbg_probe_phase_ms": [i, C.POINTER(C.c_float), C.POINTER(u64)],
             "tbg_probe_layout": [i, i, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)],
             "tbg_probe_wdl_batch": [i, vp, u64, vp, i],
@@ -342,6 +343,10 @@ class DeviceTable:
 
     def decode(self, side: int, idx, squares):
         check(lib().tbg_decode_batch(self.handle, side, ptr(idx), idx.numel(), ptr(squares)))
+
+
+def tune_split(max_split: int):
+    check(lib().tbg_tune_split(max_split))
 
 
 def probe_tune(scratch_bytes: int):

@@ -288,6 +288,15 @@ int Engine::grid_for(uint64_t units, int per_sm) {
   return g < 1 ? 1 : (int)g;
 }
 
+// Parts per tile for a bitmap of `tiles` tiles: the smallest power of two
+// (up to max_split) that gives every SM `per_sm` blocks.
+int Engine::split_for(uint64_t tiles, int per_sm) {
+  const uint64_t want = (uint64_t)num_sms * per_sm;
+  int sp = 1;
+  while (sp < max_split && tiles * sp < want) sp <<= 1;
+  return sp;
+}
+
 int Engine::check_launch(const char *what) {
   launches++;
   cudaError_t e = cudaGetLastError();
@@ -467,18 +476,25 @@ static int launch_op(const Op &o) {
   const int ns = o.ns;
   cudaStream_t st = g_eng.stream;
   switch (o.kind) {
-  case OP_SCATTER:
-    NS_SWITCH(ns, k_predecessors<NS><<<g_eng.grid_for(o.ntiles, g_eng.bps_scatter), kThreads, 0, st>>>(
-                      o.J, g_eng.d_status));
+  case OP_SCATTER: {
+    const int sp = g_eng.split_for(o.ntiles, g_eng.bps_scatter);
+    NS_SWITCH(ns, k_predecessors<NS><<<g_eng.grid_for((uint64_t)o.ntiles * sp, g_eng.bps_scatter),
+                                       kThreads, 0, st>>>(o.J, g_eng.d_status, sp));
     return g_eng.check_launch("k_predecessors");
-  case OP_SCATTER_SUB:
-    NS_SWITCH(ns, k_predecessors_sub<NS><<<g_eng.grid_for(o.ntiles, g_eng.bps_scatter), kThreads, 0,
-                                           st>>>(o.J, g_eng.d_status));
+  }
+  case OP_SCATTER_SUB: {
+    const int sp = g_eng.split_for(o.ntiles, g_eng.bps_scatter);
+    NS_SWITCH(ns, k_predecessors_sub<NS><<<g_eng.grid_for((uint64_t)o.ntiles * sp, g_eng.bps_scatter),
+                                           kThreads, 0, st>>>(o.J, g_eng.d_status, sp));
     return g_eng.check_launch("k_predecessors_sub");
-  case OP_VERIFY:
-    NS_SWITCH(ns, k_check_successors<NS><<<g_eng.grid_for(o.ntiles, g_eng.bps_verify), kThreads, 0,
-                                           st>>>(o.J, g_eng.d_status, o.out, o.out_words));
+  }
+  case OP_VERIFY: {
+    const int sp = g_eng.split_for(o.ntiles, g_eng.bps_verify);
+    NS_SWITCH(ns, k_check_successors<NS><<<g_eng.grid_for((uint64_t)o.ntiles * sp, g_eng.bps_verify),
+                                           kThreads, 0, st>>>(o.J, g_eng.d_status, o.out,
+                                                              o.out_words, sp));
     return g_eng.check_launch("k_check_successors");
+  }
   case OP_EPILOGUE: {
     uint64_t n16 = o.n16;
     k_epilogue_W<<<g_eng.grid_for((n16 + kThreads - 1) / kThreads, 8), kThreads, 0, st>>>(
@@ -962,6 +978,13 @@ extern "C" int tbg_alloc(size_t bytes, void **dev) {
 extern "C" int tbg_free(void *dev) {
   if (!dev) return TBG_OK;
   CK(cudaFree(dev));
+  return TBG_OK;
+}
+
+extern "C" int tbg_tune_split(int max_split) {
+  if (max_split < 1 || max_split > 64 || (max_split & (max_split - 1)))
+    return fail(TBG_ERR_ARG, "max_split must be a power of two from 1 to 64");
+  g_eng.max_split = max_split;
   return TBG_OK;
 }
 

@@ -84,12 +84,14 @@ struct Engine {
   uint64_t launches = 0;  // kernels launched by this library
   int bps_scatter = 8;    // grid = SMs x this for the sparse kernels (tiles loop)
   int bps_verify = 8;
+  int max_split = 64;     // parts per tile for small bitmaps (tbg_tune_split)
   Batch batch;
 
   int ensure_device();
   int add_material(const int *pt, int num);
   int fill_job(SliceJob &J, int stm, int s, bool need_sub);
   int grid_for(uint64_t units, int per_sm);
+  int split_for(uint64_t tiles, int per_sm);
   int check_launch(const char *what);
   int wait(int timeout_ms);
 };

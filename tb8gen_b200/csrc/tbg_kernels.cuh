@@ -170,7 +170,7 @@ template <class Q, class F>
 __device__ __forceinline__ void scan_tile_verify(uint64_t t, uint32_t *bits, uint64_t nbits,
                                                  uint32_t *list, uint32_t *list2, uint32_t *clr,
                                                  int *list_n, int *n2, Q &&quick, F &&full,
-                                                 uint32_t *out) {
+                                                 uint32_t *out, int lo = 0, int hi = kTileWords) {
   const uint64_t nwords = (nbits + 31) >> 5;
   const uint64_t w0 = t * kTileWords + threadIdx.x * 4;
   uint32_t w[4];
@@ -182,10 +182,12 @@ __device__ __forceinline__ void scan_tile_verify(uint64_t t, uint32_t *bits, uin
     for (int i = 0; i < 4; i++) w[i] = w0 + i < nwords ? bits[w0 + i] : 0u;
   }
   uint32_t raw[4] = {w[0], w[1], w[2], w[3]};
+  const bool mine = threadIdx.x * 4 >= lo && threadIdx.x * 4 < hi;  // the part's words
 #pragma unroll
   for (int i = 0; i < 4; i++) {
     uint64_t base = (w0 + i) * 32;
     if (base + 32 > nbits) w[i] &= base < nbits ? (1u << (nbits - base)) - 1u : 0u;
+    if (!mine) w[i] = 0;
     clr[threadIdx.x * 4 + i] = 0;
   }
   const uint64_t tbase = t * (uint64_t)kTileWords * 32;
@@ -209,7 +211,9 @@ __device__ __forceinline__ void scan_tile_verify(uint64_t t, uint32_t *bits, uin
     if (!__syncthreads_or((w[0] | w[1] | w[2] | w[3]) != 0)) break;
   }
   __syncthreads();
-  if (out != nullptr) {
+  if (!mine) {
+    // another part of the tile owns these words
+  } else if (out != nullptr) {
     if (w0 + 4 <= nwords) {
       uint4 v = make_uint4(raw[0] & ~clr[threadIdx.x * 4], raw[1] & ~clr[threadIdx.x * 4 + 1],
                            raw[2] & ~clr[threadIdx.x * 4 + 2], raw[3] & ~clr[threadIdx.x * 4 + 3]);
@@ -232,7 +236,8 @@ __device__ __forceinline__ void scan_tile_verify(uint64_t t, uint32_t *bits, uin
 template <bool kClear, bool kContig, class F, class B = NoHook, class E = NoHook>
 __device__ __forceinline__ void scan_tile(uint64_t t, uint32_t *bits, uint64_t nbits,
                                           uint32_t *list, uint32_t *clr, int *list_n, F &&f,
-                                          uint32_t *out = nullptr, B begin = B(), E end = E()) {
+                                          uint32_t *out = nullptr, B begin = B(), E end = E(),
+                                          int lo = 0, int hi = kTileWords) {
   const uint64_t nwords = (nbits + 31) >> 5;
   const int lane = threadIdx.x & 31;
   const uint64_t w0 = t * kTileWords + threadIdx.x * 4;
@@ -245,10 +250,12 @@ __device__ __forceinline__ void scan_tile(uint64_t t, uint32_t *bits, uint64_t n
     for (int i = 0; i < 4; i++) w[i] = w0 + i < nwords ? bits[w0 + i] : 0u;
   }
   uint32_t raw[4] = {w[0], w[1], w[2], w[3]};
+  const bool mine = threadIdx.x * 4 >= lo && threadIdx.x * 4 < hi;  // the part's words
 #pragma unroll
   for (int i = 0; i < 4; i++) {
     uint64_t base = (w0 + i) * 32;
     if (base + 32 > nbits) w[i] &= base < nbits ? (1u << (nbits - base)) - 1u : 0u;
+    if (!mine) w[i] = 0;
   }
   if (kClear) {
 #pragma unroll
@@ -300,7 +307,9 @@ __device__ __forceinline__ void scan_tile(uint64_t t, uint32_t *bits, uint64_t n
   end(t);
   if (kClear) {
     __syncthreads();
-    if (out != nullptr) {
+    if (!mine) {
+      // another part of the tile owns these words
+    } else if (out != nullptr) {
       if (w0 + 4 <= nwords) {
         uint4 v = make_uint4(raw[0] & ~clr[threadIdx.x * 4], raw[1] & ~clr[threadIdx.x * 4 + 1],
                              raw[2] & ~clr[threadIdx.x * 4 + 2], raw[3] & ~clr[threadIdx.x * 4 + 3]);
@@ -515,7 +524,8 @@ struct SparseSmem {
 // One tile of predecessors_worker (tb8gen.c:484-516).
 template <int NS>
 __device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem &S, uint64_t t,
-                                                  DevStatus *st) {
+                                                  DevStatus *st, int lo = 0,
+                                                  int hi = kTileWords) {
   const DMat &M = c_mats[J.mat];
   const uint64_t self_words = (M.ii.size + 31) >> 5;
   Window W{S.win, 0};
@@ -534,17 +544,33 @@ __device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem 
         window_clear(S.win);
         W.base = (int64_t)(tt * (uint64_t)kTileWords * 32) - kWinLead;
       },
-      [&](uint64_t) { window_flush(S.win, W.base, J.self, self_words); });
+      [&](uint64_t) { window_flush(S.win, W.base, J.self, self_words); }, lo, hi);
+}
+
+// A tile of a small bitmap is cut into `nsplit` parts of consecutive words
+// (nsplit a power of two up to 64), one block each, so that a bitmap of few
+// tiles still occupies every SM; each part keeps its own words' results.
+__device__ __forceinline__ void part_of(uint64_t u, int nsplit, uint64_t &t, int &lo, int &hi) {
+  t = u / (uint64_t)nsplit;
+  const int r = (int)(u % (uint64_t)nsplit);
+  lo = r * (kTileWords / nsplit);
+  hi = lo + kTileWords / nsplit;
 }
 
 template <int NS>
-__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors(SliceJob J, DevStatus *st) {
+__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors(SliceJob J, DevStatus *st,
+                                                                            int nsplit) {
   __shared__ SparseSmem S;
   load_dests(J, S.kd);
   load_binomials(S.bin);
   __syncthreads();
-  const uint64_t nt = tiles_of(J.nbits);
-  for (uint64_t t = blockIdx.x; t < nt; t += gridDim.x) tile_predecessors<NS>(J, S, t, st);
+  const uint64_t nu = tiles_of(J.nbits) * (uint64_t)nsplit;
+  for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
+    uint64_t t;
+    int lo, hi;
+    part_of(u, nsplit, t, lo, hi);
+    tile_predecessors<NS>(J, S, t, st, lo, hi);
+  }
 }
 
 // predecessors_sub_worker (tb8gen.c:346-394): the source is the sub bitmap
@@ -552,7 +578,8 @@ __global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors(Sli
 // king and by every non-king piece of stm.
 template <int NS>
 __device__ __forceinline__ void tile_predecessors_sub(const SliceJob &J, SparseSmem &S,
-                                                      uint64_t t, DevStatus *st) {
+                                                      uint64_t t, DevStatus *st, int lo = 0,
+                                                      int hi = kTileWords) {
   const DMat &M = c_mats[J.mat];
   const int kc = J.set;
   const DIdx &X = M.capt[kc];
@@ -569,17 +596,24 @@ __device__ __forceinline__ void tile_predecessors_sub(const SliceJob &J, SparseS
                            mark_king_unmoves<NS>(J, S.kd, M, S.bin, set, occ, kc, bit(me), st);
                            mark_piece_unmoves<NS>(J, M, S.bin, set, occ, kc, W, st);
                            return false;
-                         });
+                         },
+                         nullptr, NoHook(), NoHook(), lo, hi);
 }
 
 template <int NS>
-__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors_sub(SliceJob J, DevStatus *st) {
+__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors_sub(SliceJob J, DevStatus *st,
+                                                                                int nsplit) {
   __shared__ SparseSmem S;
   load_dests(J, S.kd);
   load_binomials(S.bin);
   __syncthreads();
-  const uint64_t nt = tiles_of(J.nbits);
-  for (uint64_t t = blockIdx.x; t < nt; t += gridDim.x) tile_predecessors_sub<NS>(J, S, t, st);
+  const uint64_t nu = tiles_of(J.nbits) * (uint64_t)nsplit;
+  for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
+    uint64_t t;
+    int lo, hi;
+    part_of(u, nsplit, t, lo, hi);
+    tile_predecessors_sub<NS>(J, S, t, st, lo, hi);
+  }
 }
 
 // ----------------------------------------------------------- L step
@@ -738,7 +772,8 @@ __device__ __forceinline__ bool survives_quick(const SliceJob &J, const DMat &M,
 // by the block that owns tile 0).
 template <int NS>
 __device__ __forceinline__ void tile_check(const SliceJob &J, SparseSmem &S, uint64_t t,
-                                           DevStatus *st, uint32_t *out, uint64_t out_words) {
+                                           DevStatus *st, uint32_t *out, uint64_t out_words,
+                                           int lo = 0, int hi = kTileWords) {
   const DMat &M = c_mats[J.mat];
   bb set[NS];
   RowCache rc;
@@ -752,8 +787,8 @@ __device__ __forceinline__ void tile_check(const SliceJob &J, SparseSmem &S, uin
         bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
         return refute<NS>(J, S.kd, M, S.bin, set, occ, rc, st);
       },
-      out);
-  if (out != nullptr && t == 0) {
+      out, lo, hi);
+  if (out != nullptr && t == 0 && lo == 0) {
     for (uint64_t w = ((J.nbits + 31) >> 5) + threadIdx.x; w < out_words; w += blockDim.x)
       out[w] = J.cand[w];
   }
@@ -762,13 +797,18 @@ __device__ __forceinline__ void tile_check(const SliceJob &J, SparseSmem &S, uin
 template <int NS>
 __global__ void __launch_bounds__(kThreads, TBG_MINB_VERIFY) k_check_successors(SliceJob J, DevStatus *st,
                                                                   uint32_t *out,
-                                                                  uint64_t out_words) {
+                                                                  uint64_t out_words, int nsplit) {
   __shared__ SparseSmem S;
   load_dests(J, S.kd);
   load_binomials(S.bin);
   __syncthreads();
-  const uint64_t nt = tiles_of(J.nbits);
-  for (uint64_t t = blockIdx.x; t < nt; t += gridDim.x) tile_check<NS>(J, S, t, st, out, out_words);
+  const uint64_t nu = tiles_of(J.nbits) * (uint64_t)nsplit;
+  for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
+    uint64_t t;
+    int lo, hi;
+    part_of(u, nsplit, t, lo, hi);
+    tile_check<NS>(J, S, t, st, out, out_words, lo, hi);
+  }
 }
 
 // ------------------------------------------------ dense per-position kernels
