@@ -72,6 +72,26 @@ __device__ __forceinline__ uint64_t rank_mod(const DIdx &X, const uint32_t *bin,
   return idx;
 }
 
+// The set holding square sq (-1 if none), and set[l] for a run-time l,
+// without indexing the register array at run time.
+template <int NS>
+__device__ __forceinline__ int set_of(const bb *set, int sq) {
+  int l = -1;
+#pragma unroll
+  for (int q = 0; q < NS; q++)
+    if ((set[q] >> sq) & 1) l = q;
+  return l;
+}
+
+template <int NS>
+__device__ __forceinline__ bb set_at(const bb *set, int l) {
+  bb v = 0;
+#pragma unroll
+  for (int q = 0; q < NS; q++)
+    if (q == l) v = set[q];
+  return v;
+}
+
 __device__ __forceinline__ void report(DevStatus *st, unsigned code, unsigned where,
                                        unsigned long long info) {
   if (atomicCAS(&st->err, 0u, code) == 0u) {
@@ -698,14 +718,12 @@ __device__ __forceinline__ bool refute(const SliceJob &J, const KingDest *kd, co
         bb caps = piece_attacks(M.set_type[k], x, occ) & occ & ~own & ~bit(opp);
         while (caps) {
           int to = pop_lsb(caps);
-#pragma unroll
-          for (int l = 0; l < NS; l++) {
-            if (set[l] & bit(to)) {
-              uint64_t i = rank_mod<NS>(M.capt[l], bin, J.k0, J.k1, set, k, bit(x) | bit(to), l,
+          // one rank site for every captured set (keeps the code small)
+          const int l = set_of<NS>(set, to);
+          if (l < 0) continue;
+          uint64_t i = rank_mod<NS>(M.capt[l], bin, J.k0, J.k1, set, k, bit(x) | bit(to), l,
                                     bit(to), 0, 0);
-              if (!test_sub(J.self_sub, J.self_sub_len, M.sub_offset[l], i, st)) return true;
-            }
-          }
+          if (!test_sub(J.self_sub, J.self_sub_len, M.sub_offset[l], i, st)) return true;
         }
       }
     }
@@ -717,14 +735,11 @@ __device__ __forceinline__ bool refute(const SliceJob &J, const KingDest *kd, co
     const KingDest &D = kd[d];
     if (!(occ & bit(D.to))) continue;
     if (own & bit(D.to)) continue;
-#pragma unroll
-    for (int l = 0; l < NS; l++) {
-      if (set[l] & bit(D.to)) {
-        uint64_t i = rank_mod<NS>(M.capt[l], bin, D.k0, D.k1, set, -1, 0, l,
-                              bit(msb64(set[l])), D.mirror, D.flip);
-        if (!test_sub(D.sub, D.sub_len, M.sub_offset[l], i, st)) return true;
-      }
-    }
+    const int l = set_of<NS>(set, D.to);
+    if (l < 0) continue;
+    uint64_t i = rank_mod<NS>(M.capt[l], bin, D.k0, D.k1, set, -1, 0, l,
+                              bit(msb64(set_at<NS>(set, l))), D.mirror, D.flip);
+    if (!test_sub(D.sub, D.sub_len, M.sub_offset[l], i, st)) return true;
   }
   // 5. quiet king moves into the neighbouring slices' "wins"
   for (int d = 0; d < J.nk; d++) {
