@@ -119,6 +119,18 @@ int tbg_tune_split(int max_split);
 int tbg_copy_to_device(void *dev, const void *host, size_t bytes);
 int tbg_copy_to_host(void *host, const void *dev, size_t bytes);
 
+/* The same copies queued on the library's stream without waiting (ordered
+ * with the kernels there; the host memory must stay untouched until a
+ * tbg_sync).  From page-locked memory (tbg_host_alloc) they run at full
+ * link speed. */
+int tbg_copy_to_device_async(void *dev, const void *host, size_t bytes);
+int tbg_copy_to_host_async(void *host, const void *dev, size_t bytes);
+
+/* Page-locked host memory for a host tier (TBG_ERR_NOMEM when the host
+ * cannot lock that much; fall back to ordinary memory then). */
+int tbg_host_alloc(size_t bytes, void **host);
+int tbg_host_free(void *host);
+
 /* ---- slot map (kslice_slot / kslice_buf / kslice_sub_buf) ------------ */
 
 /* Binds a device bitmap of `bytes` bytes to slice s of the current

@@ -996,6 +996,38 @@ extern "C" int tbg_copy_to_device(void *dev, const void *host, size_t bytes) {
   return TBG_OK;
 }
 
+extern "C" int tbg_copy_to_device_async(void *dev, const void *host, size_t bytes) {
+  if (!dev || !host) return fail(TBG_ERR_ARG, "null pointer");
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, g_eng.stream));
+  return TBG_OK;
+}
+
+extern "C" int tbg_copy_to_host_async(void *host, const void *dev, size_t bytes) {
+  if (!dev || !host) return fail(TBG_ERR_ARG, "null pointer");
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, g_eng.stream));
+  return TBG_OK;
+}
+
+extern "C" int tbg_host_alloc(size_t bytes, void **host) {
+  if (!host || bytes == 0) return fail(TBG_ERR_ARG, "bad allocation request");
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  *host = nullptr;
+  cudaError_t e = cudaHostAlloc(host, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(TBG_ERR_NOMEM, "cudaHostAlloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  return TBG_OK;
+}
+
+extern "C" int tbg_host_free(void *host) {
+  if (!host) return TBG_OK;
+  CK(cudaFreeHost(host));
+  return TBG_OK;
+}
+
 extern "C" int tbg_copy_to_host(void *host, const void *dev, size_t bytes) {
   if (!dev || !host) return fail(TBG_ERR_ARG, "null pointer");
   if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");

@@ -189,16 +189,33 @@ static double now_ms(void)
  * kslice.c:317-379), through the library's stream. */
 static uint64_t g_h2d_bytes, g_d2h_bytes;
 
+/* Copies are queued on the library's stream, in order with the kernels;
+ * the host reads a plane only after tbg_sync. */
 static void h2d(void *dev, const void *host, size_t n)
 {
-  ok(tbg_copy_to_device(dev, host, n), "copy to device");
+  ok(tbg_copy_to_device_async(dev, host, n), "copy to device");
   g_h2d_bytes += n;
 }
 
 static void d2h(void *host, const void *dev, size_t n)
 {
-  ok(tbg_copy_to_host(host, dev, n), "copy to host");
+  ok(tbg_copy_to_host_async(host, dev, n), "copy to host");
   g_d2h_bytes += n;
+}
+
+/* Positions set in a plane of the host tier (kslice_count over all slices),
+ * after the copies into it have finished. */
+static uint64_t plane_count(const uint8_t *plane)
+{
+  ok(tbg_sync(0), "sync");
+  uint64_t cnt = 0;
+  const uint64_t full = g_size / 64, rest = g_size % 64;
+  for (int s = 0; s < NS; s++) {
+    const uint64_t *w = (const uint64_t *)(plane + (size_t)s * g_bytes);
+    for (uint64_t i = 0; i < full; i++) cnt += (uint64_t)__builtin_popcountll(w[i]);
+    if (rest) cnt += (uint64_t)__builtin_popcountll(w[full] & ((1ULL << rest) - 1));
+  }
+  return cnt;
 }
 
 /* King-pair tables, generated from their rules (probe.c:441-539,
@@ -402,7 +419,7 @@ static void leave(int t)
 /* calc_W_n streamed (tb8gen.c:1028-1084). */
 static int st_calc_W_n(int stm, int n, int more_w)
 {
-  uint64_t cnt = 0, c;
+  uint64_t cnt = 0;
   for (int k = 0; k < NS; k++) {
     int s = order[stm][k];
     for (int j = 0; j < ntouch[stm][k]; j++) enter_target(touch[stm][k][j]);
@@ -421,13 +438,13 @@ static int st_calc_W_n(int stm, int n, int more_w)
       int t = touch[stm][k][j];
       if (last_use[stm][t] != k) continue;
       h2d(dwins, HSL(P_WINS, stm, t), g_bytes);
-      ok(tbg_epilogue_W_to(t, dwins, dwins, &c), "epilogue");
-      cnt += c;
+      ok(tbg_epilogue_W_to(t, dwins, dwins, NULL), "epilogue");
       d2h(HSL(P_WC, stm, t), wbuf[where_[t]], g_bytes);
       d2h(HSL(P_WINS, stm, t), dwins, g_bytes);
       leave(t);
     }
   }
+  cnt = plane_count(HP[stm][P_WC]);
   printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
   return cnt != 0;
 }
@@ -436,7 +453,7 @@ static int st_calc_W_n(int stm, int n, int more_w)
  * plane, then the verify. */
 static int st_calc_L_n(int stm, int n, int more_l)
 {
-  uint64_t cnt = 0, c;
+  uint64_t cnt = 0;
   for (int k = 0; k < NS; k++) {
     int s = order[stm][k];
     for (int j = 0; j < ntouch[stm][k]; j++) enter_target(touch[stm][k][j]);
@@ -482,21 +499,23 @@ static int st_calc_L_n(int stm, int n, int more_l)
     h2d(dsrc, HSL(P_X, stm, s), g_bytes);
     ok(tbg_slot_bind(-1, dsrc, g_bytes), "bind");
     ok(tbg_check_successors(stm, s), "check_successors");
-    ok(tbg_count(-1, &c), "count");
-    cnt += c;
     d2h(HSL(P_LC, stm, s), dsrc, g_bytes);
     for (int j = 0; j < ntouch[stm][k]; j++) {
       int t = touch[stm][k][j];
       if (last_use[stm][t] == k) leave(t);
     }
   }
+  cnt = plane_count(HP[stm][P_LC]);
   printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
   return cnt != 0;
 }
 
+/* Host-tier planes: page-locked while the host allows, else ordinary. */
 static void *host_alloc(size_t n)
 {
-  void *p = malloc(n);
+  void *p = NULL;
+  if (tbg_host_alloc(n, &p) == TBG_OK) return p;
+  p = malloc(n);
   if (!p) {
     fprintf(stderr, "tbgen: out of host memory (%zu bytes)\n", n);
     exit(EXIT_FAILURE);
