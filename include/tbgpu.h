@@ -346,6 +346,23 @@ int tbg_decode_batch(int handle, int side, const uint64_t *dev_idx, uint64_t n,
 int tbg_gen_positions(const char *material, uint64_t seed, uint64_t n, void *dev_queries,
                       uint32_t *failed);
 
+/* calc_sub_worker (tb8gen.c:280-314) for slice s with the 7-piece values
+ * taken from the tables of the capture materials instead of the seeded
+ * stub: handles[k] is an open table (tbg_probe_open) of the material left
+ * when one piece of set k is captured (tbg_capture_material names it; only
+ * the sets of colour stm are used).  mode 0 probes the tables (grouped rANS
+ * decode on the GPU); mode 1 evaluates the tables' defining formula with
+ * (seed, modulus) -- the values tbg_table_build stores -- without reading
+ * them (handles may be NULL).  Both give the same bitmaps.  Outputs as for
+ * tbg_calc_sub. */
+int tbg_calc_sub_table(int stm, int s, void *const dev_cls[5], const int handles[6], int mode,
+                       uint64_t seed, int modulus);
+
+/* The material left when one piece of set `set` of the current material is
+ * captured, as a name ("KRRvKRRR"), the material of the table that
+ * tbg_calc_sub_table needs for that set. */
+int tbg_capture_material(int set, char *name, int len);
+
 /* ---- synthetic inputs (no counterpart in the reference) -------------- */
 
 /* Seeded Bernoulli bitmap: bit i < nbits set iff the (i+1)-th output of the

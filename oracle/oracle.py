@@ -218,6 +218,7 @@ def ref_lib(nthreads: int = 1):
         vp, u64, i = C.c_void_p, C.c_uint64, C.c_int
         L.ref_setup.argtypes = [C.c_char_p, i]
         L.ref_set_stub.argtypes = [u64, i]
+        L.ref_set_stub_table.argtypes = [u64, i]
         L.ref_bind.argtypes = [i, vp, vp]
         L.ref_predecessors.argtypes = [i, i]
         L.ref_check_successors.argtypes = [i, i]
@@ -293,6 +294,12 @@ class Ref:
 
     def set_stub(self, seed, modulus=3):
         self.L.ref_set_stub(seed, modulus)
+
+    def set_stub_table(self, seed, modulus=3):
+        """probe_wdl answers with the value a synthetic table of the
+        position's material stores (its formula at the reference's own
+        encode_piece index) instead of the key stub."""
+        self.L.ref_set_stub_table(seed, modulus)
 
     def bind(self, s, bitmap, sub=None):
         self._keep[s] = (bitmap, sub)

@@ -57,11 +57,89 @@ static uint64_t h_mix64(uint64_t z)
 static constexpr uint64_t H_GAMMA = 0x9e3779b97f4a7c15ULL;
 static constexpr uint64_t H_STM_KEY = 0xd1b54a32d192ed03ULL;
 
+/* ---- table-formula stub ----------------------------------------------
+ * The value a synthetic table of the engine stores for the position:
+ * VALS[mix64(seed ^ idx ^ bside << 63) % modulus], idx = the reference's own
+ * encode_piece (probe.c:603-699) of the position under the table's piece
+ * layout (the kings; unless only the kings are unique, the first other
+ * unique piece in piece order; then the rest in piece order), bside/flip as
+ * probe_table chooses them for a table of the position's own material
+ * (probe.c:1554-1580).  Used to pin capture classification through tables. */
+size_t set_enc_info(struct EncInfo *ei, struct BaseEntry *be, const uint8_t *tb, int shift,
+                    int fr, const int enc);
+static int h_table_mode = 0;
+
+static int table_formula_wdl(Position *pos)
+{
+  static const int order[16] = { 0, 0, 3, 5, 7, 9, 1, 0, 0, 0, 4, 6, 8, 10, 2, 0 };
+  int n = pos->num, cnt[16] = { 0 };
+  uint8_t pt[8];
+  for (int i = 0; i < n; i++) {
+    pt[i] = pos->pt[i];
+    cnt[pos->pt[i]]++;
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = i + 1; j < n; j++)
+      if (order[pt[i]] > order[pt[j]]) {
+        uint8_t t = pt[i];
+        pt[i] = pt[j];
+        pt[j] = t;
+      }
+  int uniq = 0;
+  for (int i = 0; i < 16; i++) uniq += cnt[i] == 1;
+  bool symmetric = true;
+  for (int t = 1; t <= 6; t++) symmetric = symmetric && cnt[t] == cnt[t + 8];
+  uint8_t table[8], used[8] = { 0 };
+  int k = 0;
+  table[k++] = 6;
+  table[k++] = 14;
+  used[0] = used[1] = 1;
+  if (uniq != 2)
+    for (int i = 2; i < n; i++)
+      if (cnt[pt[i]] == 1) {
+        table[k++] = pt[i];
+        used[i] = 1;
+        break;
+      }
+  for (int i = 2; i < n; i++)
+    if (!used[i]) table[k++] = pt[i];
+  uint8_t hdr[9] = { 0 };
+  for (int i = 0; i < n; i++) hdr[1 + i] = table[i] | (table[i] << 4);
+  struct BaseEntry be;
+  memset(&be, 0, sizeof be);
+  be.num = n;
+  be.kk_enc = uniq == 2;
+  be.symmetric = symmetric;
+  struct EncInfo ei;
+  memset(&ei, 0, sizeof ei);
+  set_enc_info(&ei, &be, hdr, 0, 0, PIECE_ENC);
+  bool flip = symmetric ? pos->stm != WHITE : false;
+  int bside = symmetric ? 0 : pos->stm == BLACK;
+  uint8_t p[8] = { 0 };
+  for (int i = 0; i < n;) {
+    int t = ei.pieces[i] ^ (flip << 3);
+    for (int j = 0; j < n; j++)
+      if (pos->pt[j] == t) p[i++] = pos->sq[j] ^ (flip ? 0x38 : 0x00);
+  }
+  uint64_t idx = encode_piece(p, &ei, &be);
+  uint64_t h = h_mix64(h_seed ^ idx ^ ((uint64_t)bside << 63));
+  if (h_mod == 5) return (int)(h % 5) - 2;
+  return (int)(h % 3) * 2 - 2;
+}
+
+void ref_set_stub_table(uint64_t seed, int modulus)
+{
+  h_seed = seed;
+  h_mod = modulus == 5 ? 5 : 3;
+  h_table_mode = 1;
+}
+
 int harness_probe_wdl(Position *pos, int alpha, int beta)
 {
   (void)alpha;
   (void)beta;
   if (pos->num == 2) return 0;  /* KvK, as probe_table (probe.c:1525) */
+  if (h_table_mode) return table_formula_wdl(pos);
   uint64_t key = pos->stm ? H_STM_KEY : 0;
   for (int i = 0; i < pos->num; i++)
     key ^= h_mix64((((uint64_t)pos->pt[i] << 6) | pos->sq[i]) * H_GAMMA
@@ -77,6 +155,7 @@ void ref_set_stub(uint64_t seed, int modulus)
 {
   h_seed = seed;
   h_mod = modulus == 5 ? 5 : 3;
+  h_table_mode = 0;
 }
 
 /* ---- set-up ------------------------------------------------------------ */

@@ -78,6 +78,8 @@ def lib():
             "tbg_probe_open": [vp, u64, C.c_char_p, C.POINTER(i)],
             "tbg_probe_close": [i],
             "tbg_probe_tune": [u64],
+            "tbg_calc_sub_table": [i, i, vp * 5, C.POINTER(i), i, u64, i],
+            "tbg_capture_material": [i, C.c_char_p, i],
             "tbg_tune_split": [i],
             "tbg_probe_phase_ms": [i, C.POINTER(C.c_float), C.POINTER(u64)],
             "tbg_probe_layout": [i, i, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)],
@@ -175,6 +177,21 @@ def check_successors(stm: int, s: int):
 def calc_sub(stm: int, s: int, cls):
     arr = (C.c_void_p * 5)(*[t.data_ptr() for t in cls])
     check(lib().tbg_calc_sub(stm, s, arr))
+
+
+def calc_sub_table(stm: int, s: int, cls, handles=None, mode: int = 0, seed: int = 0,
+                   modulus: int = 3):
+    """tbg_calc_sub_table: capture classes with the 7-piece values from the
+    tables of the capture materials (mode 0) or their formula (mode 1)."""
+    arr = (C.c_void_p * 5)(*[t.data_ptr() for t in cls])
+    h = None if handles is None else (C.c_int * 6)(*(list(handles) + [-1] * (6 - len(handles))))
+    check(lib().tbg_calc_sub_table(stm, s, arr, h, mode, seed, modulus))
+
+
+def capture_material(set_index: int) -> str:
+    buf = C.create_string_buffer(32)
+    check(lib().tbg_capture_material(set_index, buf, 32))
+    return buf.value.decode()
 
 
 def calc_illegal(s: int, ill_w, ill_b):

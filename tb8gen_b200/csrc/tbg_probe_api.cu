@@ -100,6 +100,25 @@ static int spec_from_name(const char *name, Spec &sp) {
   return TBG_OK;
 }
 
+// The table layout of a material (for callers outside this file): its
+// EncInfo, symmetry, the query order and the table order of its pieces.
+int sub_layout(const char *material, EncInfoP *ei, int *symmetric, uint8_t qpt[8],
+               uint8_t tpt[8], int *num) {
+  Spec sp;
+  int rc = spec_from_name(material, sp);
+  if (rc) return rc;
+  uint8_t hdr[9] = {0};
+  for (int i = 0; i < sp.num; i++) hdr[1 + i] = (uint8_t)(sp.table[i] | (sp.table[i] << 4));
+  set_enc_info(*ei, hdr, 0, sp.num, sp.kk);
+  *symmetric = sp.symmetric;
+  memcpy(qpt, sp.pt, 8);
+  memcpy(tpt, sp.table, 8);
+  *num = sp.num;
+  return TBG_OK;
+}
+
+const EncTables *enc_tables_dev() { return enc_tables_device() == TBG_OK ? d_enc : nullptr; }
+
 // ------------------------------------------------------------------ build
 // Layout of one table side's pairs data (setup_pairs / setup_rans,
 // probe.c:1179-1206, 1156-1177).
