@@ -150,6 +150,19 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(ms, world, device="cuda"):
+    """The largest per-step time over the ranks (one all-reduce; every rank
+    calls it at the same point).  One rank: unchanged."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -268,11 +281,7 @@ def run_engine(a, rank, world, local):
     launches = tbg.launches() - n0
     ms = t0.elapsed_time(t1) / a.steps
     clk = clocks.stop()
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, world)
 
     # both paths on the same recorded batch, and per-phase device times
     plain_ms = time_mode(0, max(2, a.steps // 2))
@@ -674,11 +683,7 @@ def run_probe(a, rank, world, local):
     launches = tbg.launches() - n0
     ms = e0.elapsed_time(e1) / a.steps
     clk = clocks.stop()
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, world)
     value = ps.positions * world / (ms / 1e3)
 
     # dominant kernel: the block decode (k_probe_decode), one touched block =
