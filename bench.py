@@ -173,6 +173,16 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def committed_issue(kernel):
+    """Fraction of instruction-issue slots the kernel used in its committed
+    ncu capture (profiles/traffic.json), the roofline that binds it."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return float(json.load(f)[kernel]["issue_active_frac"])
+    except Exception:
+        return None
+
+
 def committed_traffic(kernel):
     """DRAM bytes per unit (position, or block for the probe decode) of
     `kernel` from profiles/traffic.json, which records one ncu capture of a
@@ -317,6 +327,7 @@ def run_engine(a, rank, world, local):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "alg_bytes_per_launch": int(alg), "traffic": traffic,
+                "issue_active_frac": committed_issue(dom),
                 "step_alg_GBps": round(ALG_BYTES_PER_POS * positions / (ms / 1e3) / 1e9, 1),
                 "step_frac": round(ALG_BYTES_PER_POS * positions / (ms / 1e3) / 1e9 / peak, 4)}
 
@@ -698,6 +709,7 @@ def run_probe(a, rank, world, local):
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "peak_source": peak_kind, "alg_bytes_per_launch": alg,
                 "traffic": int(tr * touched) if tr else None,
+                "issue_active_frac": committed_issue("k_probe_decode"),
                 "note": "algorithmic bytes = touched blocks x 64 KiB (each read once); "
                         "the rANS steps, not HBM, bound this kernel"}
     phase = {m: {"locate_ms": round(statistics.median(s[i][0][0] for s in phases), 3),

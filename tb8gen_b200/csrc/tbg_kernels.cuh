@@ -439,54 +439,13 @@ __device__ __forceinline__ void load_dests(const SliceJob &J, KingDest *kd) {
     if (threadIdx.x == d) kd[d] = J.kd[d];
 }
 
-// Marks into the slice's own bitmap that land near the tile being scanned
-// go to a shared-memory window first and reach HBM as one atomicOr per
-// touched word when the tile ends: moves of the last (fastest-varying) set
-// stay in their row, so most marks of such moves are local.
-constexpr int kWinWords = 3072;                     // 98,304 positions, 12 KB
-constexpr int64_t kWinLead = 32768;                 // window starts one tile early
-
-struct Window {
-  uint32_t *w;      // nullptr: no window
-  int64_t base;     // first position of the window (a multiple of 32)
-};
-
-__device__ __forceinline__ void mark_self(const SliceJob &J, const DMat &M, const Window &W,
-                                          uint64_t i, DevStatus *st) {
-  if (W.w != nullptr) {
-    int64_t r = (int64_t)i - W.base;
-    if ((uint64_t)r < (uint64_t)kWinWords * 32 && i < M.ii.size) {
-      atomicOr(&W.w[r >> 5], 1u << (r & 31));
-      return;
-    }
-  }
-  mark(J.self, i, M.ii.size, st);
-}
-
-__device__ __forceinline__ void window_clear(uint32_t *win) {
-  for (int i = threadIdx.x; i < kWinWords; i += blockDim.x) win[i] = 0;
-}
-
-__device__ __forceinline__ void window_flush(uint32_t *win, int64_t base, uint32_t *bits,
-                                             uint64_t nwords) {
-  __syncthreads();
-  const int64_t w0 = base / 32;
-  for (int i = threadIdx.x; i < kWinWords; i += blockDim.x) {
-    uint32_t v = win[i];
-    int64_t gw = w0 + i;
-    if (v && gw >= 0 && (uint64_t)gw < nwords) atomicOr(bits + gw, v);
-  }
-  __syncthreads();
-}
-
 // mark_unmoves (tb8gen.c:264-276) for every non-king piece of the side to
 // move, optionally with an uncaptured piece (set kb, square taken from the
 // moving piece's origin).
 template <int NS>
 __device__ __forceinline__ void mark_piece_unmoves(const SliceJob &J, const DMat &M,
                                                    const uint32_t *bin, const bb *set,
-                                                   bb occ, int kb, const Window &W,
-                                                   DevStatus *st) {
+                                                   bb occ, int kb, DevStatus *st) {
   bb occk = bit(J.k0) | bit(J.k1);
   uint64_t idxk = 0;
 #pragma unroll
@@ -504,7 +463,7 @@ __device__ __forceinline__ void mark_piece_unmoves(const SliceJob &J, const DMat
                          occk, idxk);
           else
             i = rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), kb, bit(x), 0, 0);
-          mark_self(J, M, W, i, st);
+          mark(J.self, i, M.ii.size, st);
         }
       }
     }
@@ -530,13 +489,8 @@ struct SparseSmem {
   uint32_t bin[7 * 64];
   KingDest kd[8];
   uint32_t list[kListCap];
-  union {
-    uint32_t win[kWinWords];   // scatter: the staging window
-    struct {
-      uint32_t clr[kTileWords];   // verify: cleared candidates of the tile
-      uint32_t list2[kListCap];   // verify: survivors of the quick test
-    };
-  };
+  uint32_t clr[kTileWords];     // verify: cleared candidates of the tile
+  uint32_t list2[kListCap];     // verify: survivors of the quick test
   int list_n;
   int n2;
 };
@@ -547,8 +501,6 @@ __device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem 
                                                   DevStatus *st, int lo = 0,
                                                   int hi = kTileWords) {
   const DMat &M = c_mats[J.mat];
-  const uint64_t self_words = (M.ii.size + 31) >> 5;
-  Window W{S.win, 0};
   bb set[NS];
   RowCache rc;
   scan_tile<false, true>(
@@ -556,15 +508,10 @@ __device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem 
       [&](uint64_t idx) {
         bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
         mark_king_unmoves<NS>(J, S.kd, M, S.bin, set, occ, -1, 0, st);
-        mark_piece_unmoves<NS>(J, M, S.bin, set, occ, -1, W, st);
+        mark_piece_unmoves<NS>(J, M, S.bin, set, occ, -1, st);
         return false;
       },
-      nullptr,
-      [&](uint64_t tt) {
-        window_clear(S.win);
-        W.base = (int64_t)(tt * (uint64_t)kTileWords * 32) - kWinLead;
-      },
-      [&](uint64_t) { window_flush(S.win, W.base, J.self, self_words); }, lo, hi);
+      nullptr, NoHook(), NoHook(), lo, hi);
 }
 
 // A tile of a small bitmap is cut into `nsplit` parts of consecutive words
@@ -603,7 +550,6 @@ __device__ __forceinline__ void tile_predecessors_sub(const SliceJob &J, SparseS
   const DMat &M = c_mats[J.mat];
   const int kc = J.set;
   const DIdx &X = M.capt[kc];
-  const Window W{nullptr, 0};
   bb set[NS];
   RowCache rc;
   scan_tile<false, true>(t, const_cast<uint32_t *>(J.src), J.nbits, S.list, nullptr, &S.list_n,
@@ -614,7 +560,7 @@ __device__ __forceinline__ void tile_predecessors_sub(const SliceJob &J, SparseS
                                attacked_by<NS>(M, set, J.k0, J.k1, occ, me, J.stm ^ 1))
                              return false;
                            mark_king_unmoves<NS>(J, S.kd, M, S.bin, set, occ, kc, bit(me), st);
-                           mark_piece_unmoves<NS>(J, M, S.bin, set, occ, kc, W, st);
+                           mark_piece_unmoves<NS>(J, M, S.bin, set, occ, kc, st);
                            return false;
                          },
                          nullptr, NoHook(), NoHook(), lo, hi);
