@@ -72,6 +72,98 @@ __device__ __forceinline__ uint64_t rank_mod(const DIdx &X, const uint32_t *bin,
   return idx;
 }
 
+// ------------------------------------------------------- incremental ranks
+// A position's index is the sum over its sets of each set's combinatorial
+// rank among the squares left free by the kings and the sets before it,
+// times the set's factor (sq_to_idx_helper, tb8gen.c:129-149).  When one
+// piece moves from a to b (or a king does, with no normalising transform),
+// a later set's rank changes only if one of its squares lies strictly
+// between a and b: only those squares change their count of occupied
+// squares below them.  The kernels keep each set's share and recompute
+// only the shares that change.
+
+// Squares strictly between a and b (a != b).
+__device__ __forceinline__ bb between(int a, int b) {
+  const int lo = a < b ? a : b, hi = a < b ? b : a;
+  return (bit(hi) - 1) & ~((bit(lo) << 1) - 1);
+}
+
+// Rank of one set's squares among the squares not in occ.
+__device__ __forceinline__ uint32_t rank_one(bb b, bb occ, const uint32_t *bin) {
+  uint32_t s = 0;
+  int j = 1;
+  while (b) {
+    const int x = pop_lsb(b);
+    s += bin[j * 64 + x - __popcll(occ & (bit(x) - 1))];
+    j++;
+  }
+  return s;
+}
+
+template <int NS>
+struct RankCtx {
+  bb pre_occ[NS];        // kings + sets before k
+  uint64_t pre_idx[NS];  // the shares of the sets before k
+  uint64_t share[NS];    // set k's share of the index
+};
+
+template <int NS>
+__device__ __forceinline__ void rank_ctx(RankCtx<NS> &c, const DIdx &X, const uint32_t *bin,
+                                         int k0, int k1, const bb *set) {
+  bb occ = bit(k0) | bit(k1);
+  uint64_t idx = 0;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    c.pre_occ[k] = occ;
+    c.pre_idx[k] = idx;
+    c.share[k] = (uint64_t)rank_one(set[k], occ, bin) * X.factor[k];
+    idx += c.share[k];
+    occ |= set[k];
+  }
+}
+
+// Index after a piece of set k moves from x to `to` (same kings, no
+// transform).
+template <int NS>
+__device__ __forceinline__ uint64_t rank_move(const RankCtx<NS> &c, const DIdx &X,
+                                              const uint32_t *bin, const bb *set, int k, int x,
+                                              int to) {
+  uint64_t idx = 0;
+  bb occ = 0;
+  const bb betw = between(x, to);
+#pragma unroll
+  for (int j = 0; j < NS; j++) {
+    if (j < k) continue;
+    if (j == k) {
+      idx = c.pre_idx[j];
+      const bb b = set[j] ^ (bit(x) | bit(to));
+      idx += (uint64_t)rank_one(b, c.pre_occ[j], bin) * X.factor[j];
+      occ = c.pre_occ[j] | b;
+    } else {
+      idx += (set[j] & betw) ? (uint64_t)rank_one(set[j], occ, bin) * X.factor[j] : c.share[j];
+      occ |= set[j];
+    }
+  }
+  return idx;
+}
+
+// Index after a king moves from `from` to `to` with no normalising
+// transform; nk0, nk1 are the kings after the move.
+template <int NS>
+__device__ __forceinline__ uint64_t rank_king_move(const RankCtx<NS> &c, const DIdx &X,
+                                                   const uint32_t *bin, const bb *set, int nk0,
+                                                   int nk1, int from, int to) {
+  const bb betw = between(from, to);
+  bb occ = bit(nk0) | bit(nk1);
+  uint64_t idx = 0;
+#pragma unroll
+  for (int j = 0; j < NS; j++) {
+    idx += (set[j] & betw) ? (uint64_t)rank_one(set[j], occ, bin) * X.factor[j] : c.share[j];
+    occ |= set[j];
+  }
+  return idx;
+}
+
 // The set holding square sq (-1 if none), and set[l] for a run-time l,
 // without indexing the register array at run time.
 template <int NS>
@@ -413,13 +505,19 @@ template <int NS>
 __device__ __forceinline__ void mark_king_unmoves(const SliceJob &J, const KingDest *kd,
                                                   const DMat &M, const uint32_t *bin,
                                                   const bb *set, bb occ, int kb, bb xb,
-                                                  DevStatus *st) {
+                                                  DevStatus *st,
+                                                  const RankCtx<NS> *c = nullptr) {
   int opp = J.stm ? J.k0 : J.k1;
+  const int me = J.stm ? J.k1 : J.k0;
   bb dest = ~(occ | king_attacks(opp));
   for (int d = 0; d < J.nk; d++) {
     const KingDest &D = kd[d];
     if (!(dest & bit(D.to))) continue;
-    uint64_t i = rank_mod<NS>(M.ii, bin, D.k0, D.k1, set, -1, 0, kb, xb, D.mirror, D.flip);
+    uint64_t i;
+    if (c != nullptr && kb < 0 && D.mirror == 0 && D.flip == 0)
+      i = rank_king_move<NS>(*c, M.ii, bin, set, D.k0, D.k1, me, D.to);
+    else
+      i = rank_mod<NS>(M.ii, bin, D.k0, D.k1, set, -1, 0, kb, xb, D.mirror, D.flip);
     mark(D.bits, i, M.ii.size, st);
     if (D.dbl) {
       // mirror_diagonal (tb8gen.c:240-244) of the normalised position: the
@@ -445,9 +543,8 @@ __device__ __forceinline__ void load_dests(const SliceJob &J, KingDest *kd) {
 template <int NS>
 __device__ __forceinline__ void mark_piece_unmoves(const SliceJob &J, const DMat &M,
                                                    const uint32_t *bin, const bb *set,
-                                                   bb occ, int kb, DevStatus *st) {
-  bb occk = bit(J.k0) | bit(J.k1);
-  uint64_t idxk = 0;
+                                                   bb occ, int kb, DevStatus *st,
+                                                   const RankCtx<NS> *c = nullptr) {
 #pragma unroll
   for (int k = 0; k < NS; k++) {
     if (M.set_color[k] == J.stm) {
@@ -458,28 +555,15 @@ __device__ __forceinline__ void mark_piece_unmoves(const SliceJob &J, const DMat
         while (mv) {
           int to = pop_lsb(mv);
           uint64_t i;
-          if (kb < 0)
-            i = rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0, k,
-                         occk, idxk);
+          if (kb < 0 && c != nullptr)
+            i = rank_move<NS>(*c, M.ii, bin, set, k, x, to);
+          else if (kb < 0)
+            i = rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0);
           else
             i = rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), kb, bit(x), 0, 0);
           mark(J.self, i, M.ii.size, st);
         }
       }
-    }
-    // Sets below the next moving set keep their rank contribution.
-    {
-      bb b = set[k];
-      bb occ2 = occk | b;
-      uint32_t s = 0;
-      int j = 1;
-      while (b) {
-        int x = pop_lsb(b);
-        s += bin[j * 64 + x - __popcll(occk & (bit(x) - 1))];
-        j++;
-      }
-      idxk += (uint64_t)s * M.ii.factor[k];
-      occk = occ2;
     }
   }
 }
@@ -507,8 +591,10 @@ __device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem 
       t, const_cast<uint32_t *>(J.src), J.nbits, S.list, nullptr, &S.list_n,
       [&](uint64_t idx) {
         bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
-        mark_king_unmoves<NS>(J, S.kd, M, S.bin, set, occ, -1, 0, st);
-        mark_piece_unmoves<NS>(J, M, S.bin, set, occ, -1, st);
+        RankCtx<NS> c;
+        rank_ctx<NS>(c, M.ii, S.bin, J.k0, J.k1, set);
+        mark_king_unmoves<NS>(J, S.kd, M, S.bin, set, occ, -1, 0, st, &c);
+        mark_piece_unmoves<NS>(J, M, S.bin, set, occ, -1, st, &c);
         return false;
       },
       nullptr, NoHook(), NoHook(), lo, hi);
@@ -600,37 +686,10 @@ __device__ __forceinline__ bool refute(const SliceJob &J, const KingDest *kd, co
                                        const RowCache &rc, DevStatus *st) {
   const int stm = J.stm;
   const int opp = stm ? J.k0 : J.k1;
-  // rank prefixes: occupancy and index contribution of the sets below k.
-  // Set 0's is the kings alone; the last set's comes from the row cache;
-  // the ones between are computed.
-  bb pre_occ[NS];
-  uint64_t pre_idx[NS];
-  pre_occ[0] = bit(J.k0) | bit(J.k1);
-  pre_idx[0] = 0;
-  if (NS > 1) {
-    pre_occ[NS - 1] = rc.occ_head;
-    pre_idx[NS - 1] = rc.row_base;
-  }
-  if (NS > 2) {
-    bb o = pre_occ[0];
-    uint64_t ix = 0;
-#pragma unroll
-    for (int k = 0; k < NS - 2; k++) {
-      bb b = set[k];
-      bb o2 = o | b;
-      uint32_t sm = 0;
-      int j = 1;
-      while (b) {
-        int x = pop_lsb(b);
-        sm += bin[j * 64 + x - __popcll(o & (bit(x) - 1))];
-        j++;
-      }
-      ix += (uint64_t)sm * M.ii.factor[k];
-      o = o2;
-      pre_occ[k + 1] = o;
-      pre_idx[k + 1] = ix;
-    }
-  }
+  const int me = stm ? J.k1 : J.k0;
+  // each set's share of the index, for the moves below
+  RankCtx<NS> c;
+  rank_ctx<NS>(c, M.ii, bin, J.k0, J.k1, set);
   bb own = 0;
 #pragma unroll
   for (int k = 0; k < NS; k++)
@@ -645,8 +704,7 @@ __device__ __forceinline__ bool refute(const SliceJob &J, const KingDest *kd, co
         bb quiet = piece_attacks(M.set_type[k], x, occ) & ~occ;
         while (quiet) {
           int to = pop_lsb(quiet);
-          uint64_t i = rank_mod<NS>(M.ii, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0, k,
-                                pre_occ[k], pre_idx[k]);
+          uint64_t i = rank_move<NS>(c, M.ii, bin, set, k, x, to);
           if (!test(J.self, i, M.ii.size, st)) return true;
         }
       }
@@ -691,7 +749,10 @@ __device__ __forceinline__ bool refute(const SliceJob &J, const KingDest *kd, co
   for (int d = 0; d < J.nk; d++) {
     const KingDest &D = kd[d];
     if (occ & bit(D.to)) continue;
-    uint64_t i = rank_mod<NS>(M.ii, bin, D.k0, D.k1, set, -1, 0, -1, 0, D.mirror, D.flip);
+    const uint64_t i =
+        (D.mirror == 0 && D.flip == 0)
+            ? rank_king_move<NS>(c, M.ii, bin, set, D.k0, D.k1, me, D.to)
+            : rank_mod<NS>(M.ii, bin, D.k0, D.k1, set, -1, 0, -1, 0, D.mirror, D.flip);
     if (!test(D.bits, i, M.ii.size, st)) return true;
   }
   return false;
