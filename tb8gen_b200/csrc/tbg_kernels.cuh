@@ -277,7 +277,9 @@ __device__ __forceinline__ void my_share(int n, int &e0, int &e1) {
 // runs on every candidate and returns 0 (refuted), 1 (survives the quick
 // test); the survivors are compacted into list2 and full(idx) (true:
 // refuted) runs on them only.  Work per thread is then nearly uniform in the
-// first pass, and the divergent full check runs on a dense list.
+// first pass, and the divergent full check runs on a dense list, handed out
+// 32 survivors at a time to whichever warp is free (n2[0]: survivors,
+// n2[1]: next survivor to hand out).
 template <class Q, class F>
 __device__ __forceinline__ void scan_tile_verify(uint64_t t, uint32_t *bits, uint64_t nbits,
                                                  uint32_t *list, uint32_t *list2, uint32_t *clr,
@@ -313,12 +315,20 @@ __device__ __forceinline__ void scan_tile_verify(uint64_t t, uint32_t *bits, uin
       if (quick(tbase + off)) list2[atomicAdd(n2, 1)] = off;
       else atomicOr(&clr[off >> 5], 1u << (off & 31));
     }
+    if (threadIdx.x == 0) n2[1] = 0;
     __syncthreads();
     const int m = *n2;
-    my_share(m, e0, e1);
-    for (int e = e0; e < e1; e++) {
-      uint32_t off = list2[e];
-      if (full(tbase + off)) atomicOr(&clr[off >> 5], 1u << (off & 31));
+    // the full checks take uneven time: warps take 32 survivors at a time
+    for (;;) {
+      int base = 0;
+      if ((threadIdx.x & 31) == 0) base = atomicAdd(&n2[1], 32);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= m) break;
+      const int e = base + (threadIdx.x & 31);
+      if (e < m) {
+        uint32_t off = list2[e];
+        if (full(tbase + off)) atomicOr(&clr[off >> 5], 1u << (off & 31));
+      }
     }
     if (!__syncthreads_or((w[0] | w[1] | w[2] | w[3]) != 0)) break;
   }
@@ -576,7 +586,7 @@ struct SparseSmem {
   uint32_t clr[kTileWords];     // verify: cleared candidates of the tile
   uint32_t list2[kListCap];     // verify: survivors of the quick test
   int list_n;
-  int n2;
+  int n2[2];
 };
 
 // One tile of predecessors_worker (tb8gen.c:484-516).
@@ -800,7 +810,7 @@ __device__ __forceinline__ void tile_check(const SliceJob &J, SparseSmem &S, uin
   bb set[NS];
   RowCache rc;
   scan_tile_verify(
-      t, J.cand, J.nbits, S.list, S.list2, S.clr, &S.list_n, &S.n2,
+      t, J.cand, J.nbits, S.list, S.list2, S.clr, &S.list_n, S.n2,
       [&](uint64_t idx) {
         bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
         return survives_quick<NS>(J, M, S.bin, set, occ, rc, st);
