@@ -131,6 +131,31 @@ int tbg_copy_to_host_async(void *host, const void *dev, size_t bytes);
 int tbg_host_alloc(size_t bytes, void **host);
 int tbg_host_free(void *host);
 
+/* ---- host-tier copies on their own streams (no counterpart in the
+ * reference, whose worker threads read and write the slice files between
+ * run_threaded calls, kslice.c:317-379) ----------------------------------
+ * Inbound and outbound copies run on two streams of the library, apart from
+ * the library stream that runs the kernels, so a host tier can fetch the
+ * next slices and write back the last ones while the kernels run.  They are
+ * ordered by tickets: a ticket stands for a point of one stream and is live
+ * until 8192 newer tickets exist (TBG_ERR_ARG for a dead one). */
+
+/* Ticket of the library stream's current point (the work issued so far). */
+int tbg_mark(uint64_t *ticket);
+
+/* Host-to-device / device-to-host copy on the inbound / outbound stream,
+ * started after the point of ticket `after` (0: no wait; the stream keeps
+ * its order, so later copies wait as well).  bytes may be 0: a pure wait.
+ * With ticket != NULL, reports the ticket of the point after the copy. */
+int tbg_copy_in(void *dev, const void *host, size_t bytes, uint64_t after, uint64_t *ticket);
+int tbg_copy_out(void *host, const void *dev, size_t bytes, uint64_t after, uint64_t *ticket);
+
+/* Later work on the library stream waits for the ticket's point. */
+int tbg_join(uint64_t ticket);
+
+/* The host waits (bounded: timeout_ms, 0 = 600000) for the ticket's point. */
+int tbg_wait_ticket(uint64_t ticket, int timeout_ms);
+
 /* ---- slot map (kslice_slot / kslice_buf / kslice_sub_buf) ------------ */
 
 /* Binds a device bitmap of `bytes` bytes to slice s of the current
@@ -196,6 +221,13 @@ int tbg_epilogue_W_to(int s, const void *dev_wins_in, void *dev_wins_out,
 /* kslice_count(s), kslice.c:524-527 (waits, bounded). */
 int tbg_count(int s, uint64_t *cnt);
 
+/* kslice_count (kslice.c:524-527) summed over n bitmaps of the bound size
+ * at dev_base + i * stride_bytes (the slices of one plane), in one launch;
+ * no counterpart in the reference, which counts slice by slice.  dev_base
+ * 16-byte aligned, stride_bytes a multiple of 16 and at least the bitmap
+ * size, 1 <= n <= 65535.  Waits (bounded) for the count. */
+int tbg_count_strided(const void *dev_base, uint64_t stride_bytes, int n, uint64_t *cnt);
+
 /* kslice_clear(s), kslice.c:292-296. */
 int tbg_clear(int s);
 
@@ -225,8 +257,20 @@ int tbg_batch_run(int mode);
 /* Epilogue counts of the last run, in record order (waits, bounded). */
 int tbg_batch_counts(uint64_t *out, int n);
 
-/* Persistent-launch configuration: CTAs per SM, and the iteration bound of
- * a dependency wait (<= 0 keeps the current one). */
+/* Records, in a batch, the count of the bitmap bound to s (kslice_count,
+ * kslice.c:524-527) after the recorded calls that write it.  Its value comes
+ * from tbg_batch_counts[_async] in record order, among the epilogue counts.
+ * TBG_ERR_STATE outside a recording. */
+int tbg_batch_count(int s);
+
+/* Queues the copy of the first n counts of the last run into host memory
+ * on the library stream (asynchronous when host_out is page-locked); the
+ * values are there once the stream has passed this point (tbg_sync, or a
+ * ticket marked after it). */
+int tbg_batch_counts_async(uint64_t *host_out, int n);
+
+/* Persistent-launch configuration: CTAs per SM (default 4), and the
+ * iteration bound of a dependency wait (<= 0 keeps the current one). */
 int tbg_batch_tune(int ctas_per_sm, long long spin_limit);
 
 /* dst = a & ~b over `bytes` (a multiple of 16) of explicit device buffers:

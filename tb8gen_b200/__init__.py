@@ -60,6 +60,7 @@ def lib():
             "tbg_calc_mate": [i, vp, vp, vp, vp],
             "tbg_epilogue_W": [i, i, C.POINTER(u64)],
             "tbg_count": [i, C.POINTER(u64)],
+            "tbg_count_strided": [vp, u64, i, C.POINTER(u64)],
             "tbg_clear": [i],
             "tbg_sub_and_not": [i, i, i],
             "tbg_sync": [i],
@@ -227,6 +228,13 @@ def launches() -> int:
 def count(s: int) -> int:
     c = C.c_uint64()
     check(lib().tbg_count(s, C.byref(c)))
+    return c.value
+
+
+def count_strided(base, stride_bytes: int, n: int) -> int:
+    """Ones below the slice size in n bitmaps at base + i * stride_bytes."""
+    c = C.c_uint64()
+    check(lib().tbg_count_strided(ptr(base), stride_bytes, n, C.byref(c)))
     return c.value
 
 

@@ -208,6 +208,8 @@ int Engine::add_material(const int *pt, int num) {
   m.num = num;
   cudaError_t e = cudaMemcpyToSymbol(c_mats, &d, sizeof d, nmats * sizeof(DMat));
   if (e != cudaSuccess) return cuda_fail(e, "upload material");
+  // a legacy-stream upload: complete before a non-blocking stream reads it
+  CK(cudaStreamSynchronize(0));
   cur = nmats;
   return nmats++;
 }
@@ -229,6 +231,9 @@ int Engine::ensure_device() {
   int mod = 3;
   CK(cudaMemcpyToSymbol(c_stub_seed, &seed, sizeof seed));
   CK(cudaMemcpyToSymbol(c_stub_mod, &mod, sizeof mod));
+  // legacy-stream set-up, complete before any stream of the caller's
+  // (blocking or not) launches
+  CK(cudaDeviceSynchronize());
   dev_ready = true;
   return TBG_OK;
 }
@@ -319,10 +324,36 @@ int Engine::wait(int timeout_ms) {
   DevStatus st;
   CK(cudaMemcpy(&st, d_status, sizeof st, cudaMemcpyDeviceToHost));
   if (st.err) {
-    CK(cudaMemset(d_status, 0, sizeof st));
+    CK(cudaMemsetAsync(d_status, 0, sizeof st, stream));
     return fail(TBG_ERR_DEVICE, "kernel status %u at site %u (byte %llu)", st.err, st.where,
                 (unsigned long long)st.info);
   }
+  return TBG_OK;
+}
+
+int Engine::tickets_ready() {
+  if (!tick_ev.empty()) return TBG_OK;
+  CK(cudaStreamCreateWithFlags(&s_in, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&s_out, cudaStreamNonBlocking));
+  std::vector<cudaEvent_t> ev(kTickets);
+  for (auto &e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  tick_ev.swap(ev);
+  return TBG_OK;
+}
+
+int Engine::ticket_event(uint64_t t, cudaEvent_t *e) {
+  if (t == 0 || t >= next_ticket || t + kTickets < next_ticket)
+    return fail(TBG_ERR_ARG, "ticket %llu is not live (next %llu)", (unsigned long long)t,
+                (unsigned long long)next_ticket);
+  *e = tick_ev[t % kTickets];
+  return TBG_OK;
+}
+
+int Engine::issue_ticket(cudaStream_t st, uint64_t *t) {
+  const uint64_t k = next_ticket;
+  CK(cudaEventRecord(tick_ev[k % kTickets], st));
+  next_ticket++;
+  *t = k;
   return TBG_OK;
 }
 
@@ -468,7 +499,7 @@ extern "C" int tbg_unbind_all(void) {
 // Every call of the ply step becomes an Op; outside a recording it is
 // launched at once, inside one it is appended to the batch.
 static uint32_t op_tiles(const Op &o) {
-  if (o.kind == OP_EPILOGUE || o.kind == OP_CLEAR) return (uint32_t)((o.n16 + kChunk16 - 1) / kChunk16);
+  if (op_streams(o.kind)) return (uint32_t)((o.n16 + kChunk16 - 1) / kChunk16);
   return (uint32_t)((o.J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull));
 }
 
@@ -504,6 +535,10 @@ static int launch_op(const Op &o) {
   case OP_CLEAR:
     CK(cudaMemsetAsync(o.T, 0, o.n16 * 16, st));
     return TBG_OK;
+  case OP_COUNT:
+    k_count<<<g_eng.grid_for((o.n16 + kThreads - 1) / kThreads, 8), kThreads, 0, st>>>(
+        o.T, o.n16, o.nbits, o.cnt);
+    return g_eng.check_launch("k_count");
   }
   return fail(TBG_ERR_ARG, "unknown op");
 }
@@ -718,6 +753,30 @@ extern "C" int tbg_count(int s, uint64_t *cnt) {
   return TBG_OK;
 }
 
+extern "C" int tbg_count_strided(const void *dev_base, uint64_t stride_bytes, int n,
+                                 uint64_t *cnt) {
+  NEED_MAT();
+  Material &m = g_eng.mats[g_eng.cur];
+  if (!dev_base || !cnt || n < 1 || n > 65535 || !aligned16(dev_base) || stride_bytes % 16 ||
+      (n > 1 && stride_bytes < m.d.bytes))
+    return fail(TBG_ERR_ARG, "bad strided count");
+  CK(cudaMemsetAsync(g_eng.d_cnt, 0, sizeof(unsigned long long), g_eng.stream));
+  const uint64_t n16 = m.d.bytes / 16;
+  const uint64_t per = (n16 + kThreads - 1) / kThreads;
+  const uint64_t want = std::max<uint64_t>(1, (uint64_t)g_eng.num_sms * 8 / (uint64_t)n);
+  dim3 grid((unsigned)std::min(per, want), (unsigned)n);
+  k_count_strided<<<grid, kThreads, 0, g_eng.stream>>>(static_cast<const uint8_t *>(dev_base),
+                                                       stride_bytes, n16, m.d.ii.size, g_eng.d_cnt);
+  int rc = g_eng.check_launch("k_count_strided");
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(g_eng.h_cnt, g_eng.d_cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     g_eng.stream));
+  rc = g_eng.wait(0);
+  if (rc) return rc;
+  *cnt = g_eng.h_cnt[0];
+  return TBG_OK;
+}
+
 extern "C" int tbg_clear(int s) {
   NEED_MAT();
   if (s < -1 || s >= TBG_NSLICES) return fail(TBG_ERR_ARG, "bad slice");
@@ -726,6 +785,20 @@ extern "C" int tbg_clear(int s) {
   Op o = new_op(OP_CLEAR);
   o.T = reinterpret_cast<uint4 *>(m.slot[s + 1]);
   o.n16 = m.d.bytes / 16;
+  return submit(o);
+}
+
+extern "C" int tbg_batch_count(int s) {
+  NEED_MAT();
+  if (s < -1 || s >= TBG_NSLICES) return fail(TBG_ERR_ARG, "bad slice");
+  if (!g_eng.batch.recording) return fail(TBG_ERR_STATE, "tbg_batch_count records into a batch");
+  Material &m = g_eng.mats[g_eng.cur];
+  if (!m.slot[s + 1]) return fail(TBG_ERR_UNBOUND, "slice %d not bound", s);
+  Op o = new_op(OP_COUNT);
+  o.T = reinterpret_cast<uint4 *>(m.slot[s + 1]);
+  o.n16 = m.d.bytes / 16;
+  o.nbits = m.d.ii.size;
+  o.cnt_slot = g_eng.batch.ncounts++;
   return submit(o);
 }
 
@@ -793,7 +866,7 @@ namespace tbg {
 
 void Batch::clear() {
   ops.clear();
-  acc.clear();
+  bufs.clear();
   preds.clear();
   ncounts = 0;
   nsmax = 1;
@@ -833,6 +906,9 @@ static void access_of(const Op &o, Batch::Access &a) {
   case OP_CLEAR:
     a.wplain.push_back(o.T);
     break;
+  case OP_COUNT:
+    a.rd.push_back(o.T);
+    break;
   }
 }
 
@@ -840,33 +916,52 @@ static bool contains(const std::vector<const void *> &v, const void *p) {
   return p != nullptr && std::find(v.begin(), v.end(), p) != v.end();
 }
 
-// Whether op b (recorded after a) must wait for a: a write of one meets a
-// read or write of the other; two accumulating scatters commute.
-static bool conflicts(const Batch::Access &a, const Batch::Access &b) {
-  for (const void *x : a.wplain)
-    if (contains(b.rd, x) || contains(b.wplain, x) || contains(b.wacc, x)) return true;
-  for (const void *x : a.wacc)
-    if (contains(b.rd, x) || contains(b.wplain, x)) return true;
-  for (const void *x : a.rd)
-    if (contains(b.wplain, x) || contains(b.wacc, x)) return true;
-  return false;
-}
-
+// Op b (recorded after a) must wait for a when a write of one meets a read or
+// write of the other; two accumulating scatters commute.  Per buffer this
+// means: a read waits for the last outright write and the accumulations
+// since; an accumulation for the last write and the reads since; an outright
+// write for all three.  Earlier accesses are covered through those ops' own
+// waits.
 int Batch::add(Op &o) {
   Access a;
   access_of(o, a);
+  std::vector<int> dep;
+  auto need = [&](const void *x, bool rd, bool accs) {
+    if (!x) return;
+    auto it = bufs.find(x);
+    if (it == bufs.end()) return;
+    const BufState &b = it->second;
+    if (b.writer >= 0) dep.push_back(b.writer);
+    if (rd) dep.insert(dep.end(), b.readers.begin(), b.readers.end());
+    if (accs) dep.insert(dep.end(), b.accs.begin(), b.accs.end());
+  };
+  for (const void *x : a.rd) need(x, false, true);
+  for (const void *x : a.wacc) need(x, true, false);
+  for (const void *x : a.wplain) need(x, true, true);
+  std::sort(dep.begin(), dep.end());
+  dep.erase(std::unique(dep.begin(), dep.end()), dep.end());
   o.pred_off = (int)preds.size();
-  o.npred = 0;
-  for (size_t i = 0; i < ops.size(); i++)
-    if (conflicts(acc[i], a)) {
-      preds.push_back((int)i);
-      o.npred++;
-    }
-  if (o.kind != OP_EPILOGUE && o.kind != OP_CLEAR) nsmax = std::max(nsmax, o.ns);
+  o.npred = (int)dep.size();
+  preds.insert(preds.end(), dep.begin(), dep.end());
+  const int me = (int)ops.size();
+  for (const void *x : a.wplain) {
+    if (!x) continue;
+    BufState &b = bufs[x];
+    b.writer = me;
+    b.readers.clear();
+    b.accs.clear();
+  }
+  auto note = [&](const void *x, bool rd) {
+    if (!x || contains(a.wplain, x)) return;
+    std::vector<int> &v = rd ? bufs[x].readers : bufs[x].accs;
+    if (v.empty() || v.back() != me) v.push_back(me);
+  };
+  for (const void *x : a.rd) note(x, true);
+  for (const void *x : a.wacc) note(x, false);
+  if (!op_streams(o.kind)) nsmax = std::max(nsmax, o.ns);
   o.first = total;
   total += o.ntiles;
   ops.push_back(o);
-  acc.push_back(std::move(a));
   return TBG_OK;
 }
 
@@ -894,9 +989,13 @@ int Batch::finish() {
     if (e != cudaSuccess) return fail(TBG_ERR_NOMEM, "batch queue: %s", cudaGetErrorString(e));
   }
   for (Op &o : ops) o.cnt = o.cnt_slot >= 0 ? d_counts + o.cnt_slot : nullptr;
-  CK(cudaMemcpy(d_ops, ops.data(), ops.size() * sizeof(Op), cudaMemcpyHostToDevice));
+  // Stream-ordered after a run of the previous batch that may still read the
+  // queue; from pageable memory the call returns once the bytes are staged.
+  CK(cudaMemcpyAsync(d_ops, ops.data(), ops.size() * sizeof(Op), cudaMemcpyHostToDevice,
+                     g_eng.stream));
   if (!preds.empty())
-    CK(cudaMemcpy(d_preds, preds.data(), preds.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(d_preds, preds.data(), preds.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       g_eng.stream));
   ready = true;
   return TBG_OK;
 }
@@ -965,13 +1064,27 @@ extern "C" int tbg_batch_counts(uint64_t *out, int n) {
   return TBG_OK;
 }
 
+extern "C" int tbg_batch_counts_async(uint64_t *host_out, int n) {
+  Batch &b = g_eng.batch;
+  if (!b.ready || !host_out || n < 0 || n > b.ncounts) return fail(TBG_ERR_ARG, "bad count request");
+  if (n == 0) return TBG_OK;
+  CK(cudaMemcpyAsync(host_out, b.d_counts, n * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                     g_eng.stream));
+  return TBG_OK;
+}
+
 extern "C" int tbg_alloc(size_t bytes, void **dev) {
   if (!dev || bytes == 0) return fail(TBG_ERR_ARG, "bad allocation request");
   if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
   *dev = nullptr;
   cudaError_t e = cudaMalloc(dev, bytes);
   if (e != cudaSuccess) return fail(TBG_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
-  CK(cudaMemset(*dev, 0, bytes));
+  // Zeroed on a stream of its own and waited for: a plain cudaMemset would
+  // queue on the legacy default stream, unordered with the caller's
+  // non-blocking streams, and could land after the caller's first copy.
+  if (!g_eng.s_zero) CK(cudaStreamCreateWithFlags(&g_eng.s_zero, cudaStreamNonBlocking));
+  CK(cudaMemsetAsync(*dev, 0, bytes, g_eng.s_zero));
+  CK(cudaStreamSynchronize(g_eng.s_zero));
   return TBG_OK;
 }
 
@@ -1008,6 +1121,75 @@ extern "C" int tbg_copy_to_host_async(void *host, const void *dev, size_t bytes)
   if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
   CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, g_eng.stream));
   return TBG_OK;
+}
+
+// ---------------------------------------------------------- copy streams
+extern "C" int tbg_mark(uint64_t *ticket) {
+  if (!ticket) return fail(TBG_ERR_ARG, "null ticket");
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  int rc = g_eng.tickets_ready();
+  if (rc) return rc;
+  return g_eng.issue_ticket(g_eng.stream, ticket);
+}
+
+static int side_copy(cudaStream_t st, void *dst, const void *src, size_t n, cudaMemcpyKind kind,
+                     uint64_t after, uint64_t *ticket) {
+  if (after) {
+    cudaEvent_t e;
+    int rc = g_eng.ticket_event(after, &e);
+    if (rc) return rc;
+    CK(cudaStreamWaitEvent(st, e, 0));
+  }
+  if (n) CK(cudaMemcpyAsync(dst, src, n, kind, st));
+  if (ticket) return g_eng.issue_ticket(st, ticket);
+  return TBG_OK;
+}
+
+static int side_ready(size_t n, const void *a, const void *b) {
+  if (n && (!a || !b)) return fail(TBG_ERR_ARG, "null pointer");
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  return g_eng.tickets_ready();
+}
+
+extern "C" int tbg_copy_in(void *dev, const void *host, size_t bytes, uint64_t after,
+                           uint64_t *ticket) {
+  int rc = side_ready(bytes, dev, host);
+  if (rc) return rc;
+  return side_copy(g_eng.s_in, dev, host, bytes, cudaMemcpyHostToDevice, after, ticket);
+}
+
+extern "C" int tbg_copy_out(void *host, const void *dev, size_t bytes, uint64_t after,
+                            uint64_t *ticket) {
+  int rc = side_ready(bytes, dev, host);
+  if (rc) return rc;
+  return side_copy(g_eng.s_out, host, dev, bytes, cudaMemcpyDeviceToHost, after, ticket);
+}
+
+extern "C" int tbg_join(uint64_t ticket) {
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  cudaEvent_t e;
+  int rc = g_eng.ticket_event(ticket, &e);
+  if (rc) return rc;
+  CK(cudaStreamWaitEvent(g_eng.stream, e, 0));
+  return TBG_OK;
+}
+
+extern "C" int tbg_wait_ticket(uint64_t ticket, int timeout_ms) {
+  if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
+  cudaEvent_t e;
+  int rc = g_eng.ticket_event(ticket, &e);
+  if (rc) return rc;
+  auto t0 = std::chrono::steady_clock::now();
+  const long limit = timeout_ms > 0 ? timeout_ms : 600000;
+  for (;;) {
+    cudaError_t q = cudaEventQuery(e);
+    if (q == cudaSuccess) return TBG_OK;
+    if (q != cudaErrorNotReady) return cuda_fail(q, "ticket");
+    auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                  std::chrono::steady_clock::now() - t0).count();
+    if (ms > limit) return fail(TBG_ERR_TIMEOUT, "ticket not reached within %ld ms", limit);
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
 }
 
 extern "C" int tbg_host_alloc(size_t bytes, void **host) {

@@ -5,9 +5,9 @@
 // into an Op with its bindings resolved.  An Op is cut into tiles (32,768
 // positions for the sparse kernels, 1 MiB for the streaming ones); the queue
 // is the list of (op, tile) items in record order.  Each op lists the earlier
-// ops whose buffers it conflicts with (read-after-write, write-after-read,
+// ops it waits for, found per buffer (read-after-write, write-after-read,
 // write-after-write; two scatters into one bitmap commute and do not
-// conflict).  A CTA takes the next item with one atomicAdd, waits -- with an
+// conflict; the waits of the listed ops cover older accesses).  A CTA takes the next item with one atomicAdd, waits -- with an
 // iteration bound -- until the item's predecessor ops have all their tiles
 // done, runs the tile and counts it done.  Items are taken in record order,
 // so every predecessor of the earliest unfinished item was taken earlier and
@@ -28,7 +28,8 @@ __device__ __forceinline__ unsigned int load_acquire(const unsigned int *p) {
   return v;
 }
 
-// One 1 MiB chunk of the fused epilogue (k_epilogue_W) or of a clear.
+// One 1 MiB chunk of the fused epilogue (k_epilogue_W), of a clear or of a
+// count.
 __device__ __forceinline__ void tile_stream(const Op &o, uint64_t t) {
   const uint64_t i0 = t * kChunk16;
   const uint64_t i1 = i0 + kChunk16 < o.n16 ? i0 + kChunk16 : o.n16;
@@ -39,12 +40,16 @@ __device__ __forceinline__ void tile_stream(const Op &o, uint64_t t) {
   }
   unsigned long long c = 0;
   const uint64_t full16 = o.nbits >> 7;
+  const bool count_only = o.kind == OP_COUNT;
   for (uint64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-    uint4 t4 = o.T[i], w = o.win[i];
-    t4.x &= ~w.x; t4.y &= ~w.y; t4.z &= ~w.z; t4.w &= ~w.w;
-    w.x |= t4.x; w.y |= t4.y; w.z |= t4.z; w.w |= t4.w;
-    o.T[i] = t4;
-    o.wout[i] = w;
+    uint4 t4 = o.T[i];
+    if (!count_only) {
+      uint4 w = o.win[i];
+      t4.x &= ~w.x; t4.y &= ~w.y; t4.z &= ~w.z; t4.w &= ~w.w;
+      w.x |= t4.x; w.y |= t4.y; w.z |= t4.z; w.w |= t4.w;
+      o.T[i] = t4;
+      o.wout[i] = w;
+    }
     if (i < full16) {
       c += popc4(t4);
     } else if (i == full16) {
@@ -121,7 +126,7 @@ k_batch(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, uin
     }
     __syncthreads();
     const uint64_t t = s_item - so.first;
-    if (so.kind == OP_EPILOGUE || so.kind == OP_CLEAR) {
+    if (op_streams(so.kind)) {
       tile_stream(so, t);
     } else {
       load_dests(so.J, S.kd);

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <unordered_map>
 #include <vector>
 
 #include "tbg_types.h"
@@ -46,7 +47,15 @@ struct Batch {
   struct Access {
     std::vector<const void *> rd, wplain, wacc;
   };
-  std::vector<Access> acc;
+  // Per buffer: the last op that wrote it outright, and the ops that read it
+  // or accumulated into it since.  An op depends on these, not on every
+  // earlier op: a dependency wait ends only when all tiles of the awaited
+  // op are done, and those waited in turn for theirs.
+  struct BufState {
+    int writer = -1;
+    std::vector<int> readers, accs;
+  };
+  std::unordered_map<const void *, BufState> bufs;
   std::vector<int> preds;
   int ncounts = 0;
   int nsmax = 1;
@@ -62,7 +71,7 @@ struct Batch {
   size_t cap_counts = 0;
   unsigned long long *d_next = nullptr;
   // persistent launch configuration
-  int ctas_per_sm = 2;
+  int ctas_per_sm = 4;
   long long spin_limit = 50000000;
 
   void clear();
@@ -86,6 +95,13 @@ struct Engine {
   int bps_verify = 8;
   int max_split = 64;     // parts per tile for small bitmaps (tbg_tune_split)
   Batch batch;
+  // Host-tier copy streams (inbound, outbound) and the event ring behind
+  // tickets: ticket t is event t % kTickets until kTickets later ones exist.
+  static constexpr uint64_t kTickets = 8192;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaStream_t s_zero = nullptr;  // zero-fills new allocations (tbg_alloc)
+  std::vector<cudaEvent_t> tick_ev;
+  uint64_t next_ticket = 1;
 
   int ensure_device();
   int add_material(const int *pt, int num);
@@ -94,6 +110,9 @@ struct Engine {
   int split_for(uint64_t tiles, int per_sm);
   int check_launch(const char *what);
   int wait(int timeout_ms);
+  int tickets_ready();
+  int ticket_event(uint64_t t, cudaEvent_t *e);
+  int issue_ticket(cudaStream_t st, uint64_t *t);
 };
 
 extern HostTables g_tab;

@@ -1084,13 +1084,14 @@ __global__ void __launch_bounds__(kThreads) k_epilogue_W(uint4 *T, const uint4 *
   }
 }
 
-// kslice_count_addr (kslice.c:500-522): ones below nbits.
-__global__ void __launch_bounds__(kThreads) k_count(const uint4 *p, uint64_t n16, uint64_t nbits,
-                                                    unsigned long long *cnt) {
+// kslice_count_addr (kslice.c:500-522): ones below nbits, blocks blk of nblk
+// striding over the bitmap; one atomic add per block.
+__device__ __forceinline__ void count_bits(const uint4 *p, uint64_t n16, uint64_t nbits,
+                                           unsigned long long *cnt, uint64_t blk, uint64_t nblk) {
   uint64_t c = 0;
   const uint64_t full16 = nbits >> 7;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n16 && i <= full16;
-       i += (uint64_t)gridDim.x * blockDim.x) {
+  for (uint64_t i = blk * blockDim.x + threadIdx.x; i < n16 && i <= full16;
+       i += nblk * blockDim.x) {
     uint4 t = p[i];
     if (i < full16) {
       c += popc4(t);
@@ -1114,6 +1115,19 @@ __global__ void __launch_bounds__(kThreads) k_count(const uint4 *p, uint64_t n16
     for (int i = 0; i < kThreads / 32; i++) s += part[i];
     if (s) atomicAdd(cnt, s);
   }
+}
+
+__global__ void __launch_bounds__(kThreads) k_count(const uint4 *p, uint64_t n16, uint64_t nbits,
+                                                    unsigned long long *cnt) {
+  count_bits(p, n16, nbits, cnt, blockIdx.x, gridDim.x);
+}
+
+// The count over the slices of a plane: bitmap blockIdx.y at base + y * stride.
+__global__ void __launch_bounds__(kThreads) k_count_strided(const uint8_t *base, uint64_t stride,
+                                                            uint64_t n16, uint64_t nbits,
+                                                            unsigned long long *cnt) {
+  const uint4 *p = reinterpret_cast<const uint4 *>(base + (uint64_t)blockIdx.y * stride);
+  count_bits(p, n16, nbits, cnt, blockIdx.x, gridDim.x);
 }
 
 // p &= ~q over n16 vectors (kslice_sub_and_not, kslice.c:481-487).

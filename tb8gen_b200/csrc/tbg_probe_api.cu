@@ -40,6 +40,7 @@ static int enc_tables_device() {
   if (!d_enc) {
     PCK(cudaMalloc(&d_enc, sizeof(EncTables)));
     PCK(cudaMemcpy(d_enc, &g_enc, sizeof(EncTables), cudaMemcpyHostToDevice));
+    PCK(cudaStreamSynchronize(0));  // legacy-stream upload, before any stream reads it
   }
   return TBG_OK;
 }
@@ -440,6 +441,7 @@ static int open_table(const uint8_t *dev_table, uint64_t bytes, const char *mate
     PCK(cudaMemcpy(base, &ps[b].dt, sizeof(RansDecodeTab), cudaMemcpyHostToDevice));
     PCK(cudaMemcpy(base + sizeof(RansDecodeTab), ps[b].symlen.data(), ps[b].num_syms,
                    cudaMemcpyHostToDevice));
+    PCK(cudaStreamSynchronize(0));  // legacy-stream uploads, before any stream reads them
     ProbeSide &S = H.P.side[b];
     S.index = dev_table + off_index[b];
     S.sizes = dev_table + off_sizes[b];
@@ -693,8 +695,10 @@ extern "C" int tbg_gen_positions(const char *material, uint64_t seed, uint64_t n
   uint32_t *d_fail;
   PCK(cudaMalloc(&d_pt, 8));
   PCK(cudaMalloc(&d_fail, 4));
-  PCK(cudaMemcpy(d_pt, sp.pt, 8, cudaMemcpyHostToDevice));
-  PCK(cudaMemset(d_fail, 0, 4));
+  // on the launch stream: a legacy-stream copy or memset is not ordered
+  // with a non-blocking caller stream
+  PCK(cudaMemcpyAsync(d_pt, sp.pt, 8, cudaMemcpyHostToDevice, g_eng.stream));
+  PCK(cudaMemsetAsync(d_fail, 0, 4, g_eng.stream));
   k_gen_positions<<<g_eng.num_sms * 8, 256, 0, g_eng.stream>>>(sp.num, d_pt, seed, n,
                                                                static_cast<Query *>(dev_queries), d_fail);
   rc = g_eng.check_launch("k_gen_positions");

@@ -75,7 +75,14 @@ struct DevStatus {
   unsigned long long info;
 };
 
-enum OpKind : int { OP_SCATTER = 1, OP_SCATTER_SUB = 2, OP_VERIFY = 3, OP_EPILOGUE = 4, OP_CLEAR = 5 };
+enum OpKind : int {
+  OP_SCATTER = 1, OP_SCATTER_SUB = 2, OP_VERIFY = 3, OP_EPILOGUE = 4, OP_CLEAR = 5, OP_COUNT = 6
+};
+
+// The ops that stream whole bitmaps in 1 MiB chunks (the others work by tile).
+__host__ __device__ inline bool op_streams(int kind) {
+  return kind == OP_EPILOGUE || kind == OP_CLEAR || kind == OP_COUNT;
+}
 
 constexpr uint64_t kChunk16 = 1u << 16;   // streaming tile: 65,536 x 16 B = 1 MiB
 

@@ -3,7 +3,7 @@
  * calc_sub_kslices, calc_illegal_and_mate, calc_L_n, calc_W_n) as a C host
  * over the tbgpu C ABI, with every king slice resident in HBM.
  *
- *   tbgen [-s seed] [-m 3|5] [-b device_MB] [-S] [-p] [-n max_ply] MATERIAL
+ *   tbgen [-s seed] [-m 3|5] [-b device_MB] [-S] [-g steps] [-P] [-p] [-n max_ply] MATERIAL
  *
  * Prints the reference's per-ply counts ("broken_w = ...", "l<n>_<c> = ...",
  * "w<n>_<c> = ...") in the reference's order.
@@ -22,12 +22,21 @@
  * window of slices that follows the schedule's slice order, as the
  * reference's manager does: a slice is brought in before the first step
  * that unmoves into it (or reads it) and written out after the last one.
+ * The steps run in segments of -g steps (default 32 for slices up to 16 MB,
+ * else 8), pipelined: a
+ * segment's reads from the host tier and the previous segment's writes
+ * overlap the kernels of the segment between them.
+ *
+ * In resident mode each half-ply is recorded as one batch and run by the
+ * persistent kernel (tbg_batch_run mode 1); -P launches every call on its
+ * own instead, in the reference's call order.
  *
  * -p prints a timing line per half-ply ("time <kind><n>_<c> ms=...").
  * 7-piece capture values come from the seeded stub (tbg_set_stub); a capture
  * that leaves the two kings alone is a draw, as in the reference.
  */
 #define _POSIX_C_SOURCE 200809L
+#include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -110,21 +119,62 @@ static void illegal_and_mate(void)
          (unsigned long long)lb);
 }
 
+/* Half-plies of the resident mode run as one recorded batch (a persistent
+ * kernel whose work queue follows the calls' buffer dependencies) unless -P
+ * asks for one launch per call. */
+static int g_plain;
+
+static void batch_begin(void)
+{
+  if (!g_plain) ok(tbg_batch_begin(), "batch begin");
+}
+
+static void batch_run(void)
+{
+  if (g_plain) return;
+  int nops;
+  uint64_t items;
+  ok(tbg_batch_end(&nops, &items), "batch end");
+  ok(tbg_batch_run(1), "batch run");
+}
+
+/* Ones in the slices of a plane: one strided count when the slices lie at
+ * a fixed stride (the resident layout), else slice by slice. */
+static uint64_t plane_total(uint8_t *pl[NS])
+{
+  uint64_t cnt = 0, c;
+  const ptrdiff_t stride = pl[1] - pl[0];
+  int uniform = stride > 0;
+  for (int s = 1; s < NS && uniform; s++) uniform = pl[s] - pl[0] == stride * s;
+  if (uniform) {
+    ok(tbg_count_strided(pl[0], (uint64_t)stride, NS, &cnt), "count");
+    return cnt;
+  }
+  for (int s = 0; s < NS; s++) {
+    ok(tbg_slot_bind(-1, pl[s], g_bytes), "bind");
+    ok(tbg_count(-1, &c), "count");
+    cnt += c;
+  }
+  return cnt;
+}
+
 /* calc_L_n, tb8gen.c:943-1026: stm losses in n, into Lc[stm]. */
 static int calc_L_n(int stm, int n, int more_l)
 {
-  uint64_t cnt = 0, c;
+  uint64_t cnt;
+  if (n == DRAW_RULE + 1)  /* cwin \ win (tb8gen.c:964-970) */
+    for (int s = 0; s < NS; s++)
+      ok(tbg_bitmap_and_not(subtmp[s], sub[stm ^ 1][C_CWIN][s], sub[stm ^ 1][C_WIN][s], g_sub),
+         "and_not");
   /* candidates: predecessors of stm^1's W(n-1) and of its winning captures */
   bind_all(Lc[stm], NULL);
+  batch_begin();
   for (int s = 0; s < NS; s++) ok(tbg_clear(s), "clear");
   for (int s = 0; s < NS; s++) {
     if (n == 1) {
       ok(tbg_sub_bind(s, sub[stm ^ 1][C_WIN][s], g_sub), "bind sub");
       ok(tbg_predecessors_sub(stm, s, 1), "predecessors_sub");
     } else if (n == DRAW_RULE + 1) {
-      /* cwin \ win (tb8gen.c:964-970) */
-      ok(tbg_bitmap_and_not(subtmp[s], sub[stm ^ 1][C_CWIN][s], sub[stm ^ 1][C_WIN][s], g_sub),
-         "and_not");
       ok(tbg_sub_bind(s, subtmp[s], g_sub), "bind sub");
       ok(tbg_predecessors_sub(stm, s, 0), "predecessors_sub");
     }
@@ -140,11 +190,8 @@ static int calc_L_n(int stm, int n, int more_l)
     ok(tbg_slot_bind(-1, Lc[stm][s], g_bytes), "bind");
     ok(tbg_check_successors(stm, s), "check_successors");
   }
-  for (int s = 0; s < NS; s++) {
-    ok(tbg_slot_bind(-1, Lc[stm][s], g_bytes), "bind");
-    ok(tbg_count(-1, &c), "count");
-    cnt += c;
-  }
+  batch_run();
+  cnt = plane_total(Lc[stm]);
   printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
   return cnt != 0;
 }
@@ -152,8 +199,9 @@ static int calc_L_n(int stm, int n, int more_l)
 /* calc_W_n, tb8gen.c:1028-1084: stm wins in n, into Wc[stm]. */
 static int calc_W_n(int stm, int n, int more_w)
 {
-  uint64_t cnt = 0, c;
+  uint64_t cnt = 0, c[NS];
   bind_all(Wc[stm], NULL);
+  batch_begin();
   for (int s = 0; s < NS; s++) ok(tbg_clear(s), "clear");
   for (int s = 0; s < NS; s++) {
     if (n == 1 || n == DRAW_RULE + 1) {
@@ -165,14 +213,16 @@ static int calc_W_n(int stm, int n, int more_w)
       ok(tbg_predecessors(stm, s), "predecessors");
     }
   }
-  for (int s = 0; s < NS; s++) {
-    ok(tbg_epilogue_W_to(s, wins[stm][s], wins[stm][s], &c), "epilogue");
-    cnt += c;
+  for (int s = 0; s < NS; s++)
+    ok(tbg_epilogue_W_to(s, wins[stm][s], wins[stm][s], g_plain ? &c[s] : NULL), "epilogue");
+  if (!g_plain) {
+    batch_run();
+    ok(tbg_batch_counts(c, NS), "counts");
   }
+  for (int s = 0; s < NS; s++) cnt += c[s];
   printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
   return cnt != 0;
 }
-
 
 /* ------------------------------------------------------------ streamed mode */
 static uint64_t g_size;        /* positions per slice */
@@ -189,33 +239,12 @@ static double now_ms(void)
  * kslice.c:317-379), through the library's stream. */
 static uint64_t g_h2d_bytes, g_d2h_bytes;
 
-/* Copies are queued on the library's stream, in order with the kernels;
- * the host reads a plane only after tbg_sync. */
-static void h2d(void *dev, const void *host, size_t n)
-{
-  ok(tbg_copy_to_device_async(dev, host, n), "copy to device");
-  g_h2d_bytes += n;
-}
-
+/* Set-up copies are queued on the library's stream, in order with the
+ * kernels. */
 static void d2h(void *host, const void *dev, size_t n)
 {
   ok(tbg_copy_to_host_async(host, dev, n), "copy to host");
   g_d2h_bytes += n;
-}
-
-/* Positions set in a plane of the host tier (kslice_count over all slices),
- * after the copies into it have finished. */
-static uint64_t plane_count(const uint8_t *plane)
-{
-  ok(tbg_sync(0), "sync");
-  uint64_t cnt = 0;
-  const uint64_t full = g_size / 64, rest = g_size % 64;
-  for (int s = 0; s < NS; s++) {
-    const uint64_t *w = (const uint64_t *)(plane + (size_t)s * g_bytes);
-    for (uint64_t i = 0; i < full; i++) cnt += (uint64_t)__builtin_popcountll(w[i]);
-    if (rest) cnt += (uint64_t)__builtin_popcountll(w[full] & ((1ULL << rest) - 1));
-  }
-  return cnt;
 }
 
 /* King-pair tables, generated from their rules (probe.c:441-539,
@@ -350,36 +379,24 @@ static uint8_t *HP[2][NPLANE], *HS[2][5];
 #define HSL(plane, c, s) (HP[c][plane] + (size_t)(s) * g_bytes)
 #define HSUB(c, k, s) (HS[c][k] + (size_t)(s) * g_sub)
 
-/* device window */
-static uint8_t **wbuf, **wsub, *dsrc, *dwins, *dsub_src, *dsub_tmp;
-static int *wfree, nfree, where_[NS];
-
-static int take(void)
-{
-  if (nfree == 0) {
-    fprintf(stderr, "tbgen: window exhausted\n");
-    exit(EXIT_FAILURE);
-  }
-  return wfree[--nfree];
-}
-
-static void give(int b) { wfree[nfree++] = b; }
+/* device buffers of the set-up steps (calc_sub, illegal and mate) */
+static uint8_t *setup_bm[4], *setup_sub[5], *setup_base;
 
 static void st_calc_subs(void)
 {
   for (int stm = 0; stm < 2; stm++)
     for (int s = 0; s < NS; s++) {
-      void *cls[5] = { wsub[0], wsub[1], wsub[2], wsub[3], wsub[4] };
+      void *cls[5] = { setup_sub[0], setup_sub[1], setup_sub[2], setup_sub[3], setup_sub[4] };
       ok(tbg_calc_sub(stm, s, cls), "calc_sub");
-      for (int k = 0; k < 5; k++) d2h(HSUB(stm, k, s), wsub[k], g_sub);
+      for (int k = 0; k < 5; k++) d2h(HSUB(stm, k, s), setup_sub[k], g_sub);
     }
 }
 
 static void st_illegal_and_mate(void)
 {
   uint64_t cnt[4] = { 0, 0, 0, 0 }, c;
+  uint8_t **b = setup_bm;
   for (int s = 0; s < NS; s++) {
-    uint8_t *b[4] = { wbuf[0], wbuf[1], wbuf[2], wbuf[3] };
     ok(tbg_calc_illegal(s, b[0], b[1]), "illegal");
     ok(tbg_calc_mate(s, b[0], b[1], b[2], b[3]), "mate");
     for (int j = 0; j < 4; j++) {
@@ -398,53 +415,258 @@ static void st_illegal_and_mate(void)
          (unsigned long long)cnt[3]);
 }
 
-/* Brings slice t into the window for a scatter (cleared target). */
-static void enter_target(int t)
+/* ---- the pipeline of the streamed half-plies ----
+ * A part of a half-ply (the scatter of calc_W_n, the candidates of
+ * calc_L_n, or its verify) runs the schedule's steps in segments of g_seg
+ * steps, numbered across parts.  For segment q:
+ *   reads   the host-tier planes it needs go to the device on the inbound
+ *           copy stream, queued before segment q-1's kernels so that they
+ *           run meanwhile; they wait only for segment q-3's writes, the last
+ *           users of the staging set (q mod 3) and of the window buffers
+ *           released three segments back;
+ *   kernels its calls are recorded as one batch and run by the persistent
+ *           kernel on the library stream, after its reads;
+ *   writes  the slices that step their last in q go back to the host tier
+ *           on the outbound copy stream after the kernels; their window
+ *           buffers are taken again two segments later at the earliest.
+ * Slices enter the window (the reference's KSliceManager, kslice.c:41-84)
+ * before the first step that touches them and leave after the last. */
+enum { NPAR = 3, TK_RING = 8, MAX_SEG = 64 };
+static int g_seg;                              /* 0: chosen from the slice size */
+static int g_lw;                               /* most last uses in a segment */
+static int64_t g_seq;                          /* segments issued so far */
+static uint64_t in_tk[TK_RING], out_tk[TK_RING];
+static uint8_t *st_src[NPAR][MAX_SEG], *st_sub[NPAR][MAX_SEG], *st_subt[NPAR][MAX_SEG];
+static uint8_t **st_win[NPAR];
+static uint64_t *hcnt;                         /* counts of a half-ply (page-locked) */
+static int ncnt;
+
+typedef struct {
+  uint8_t *bm, *sub;
+  int64_t rel;  /* segment whose kernels used it last */
+  int used;
+} WinBuf;
+static WinBuf *win;
+static int nwin, capwin, where_[NS];
+
+/* A window buffer released at segment <= max_rel, else a new one. */
+static int take(int64_t max_rel)
 {
-  if (where_[t] >= 0) return;
-  int b = take();
-  where_[t] = b;
-  ok(tbg_slot_bind(t, wbuf[b], g_bytes), "bind");
-  ok(tbg_clear(t), "clear");
+  for (int b = 0; b < nwin; b++)
+    if (!win[b].used && win[b].rel <= max_rel) {
+      win[b].used = 1;
+      return b;
+    }
+  if (nwin == capwin) {
+    capwin = capwin ? 2 * capwin : 64;
+    win = realloc(win, capwin * sizeof *win);
+    if (!win) {
+      fprintf(stderr, "tbgen: out of host memory\n");
+      exit(EXIT_FAILURE);
+    }
+  }
+  uint8_t *p;
+  ok(tbg_alloc(g_bytes + g_sub, (void **)&p), "window buffer");
+  win[nwin] = (WinBuf){ p, p + g_bytes, INT64_MIN, 1 };
+  return nwin++;
 }
 
-static void leave(int t)
+/* After a wait that covers every earlier use: all free buffers may be taken. */
+static void reset_window(void)
+{
+  for (int b = 0; b < nwin; b++)
+    if (!win[b].used) win[b].rel = INT64_MIN;
+}
+
+static void release(int t, int64_t q)
 {
   ok(tbg_slot_bind(t, NULL, 0), "unbind");
   ok(tbg_sub_bind(t, NULL, 0), "unbind sub");
-  give(where_[t]);
+  win[where_[t]].used = 0;
+  win[where_[t]].rel = q;
   where_[t] = -1;
+}
+
+static void cin(void *dev, const void *host, size_t n)
+{
+  ok(tbg_copy_in(dev, host, n, 0, NULL), "copy in");
+  g_h2d_bytes += n;
+}
+
+static void cout_(void *host, const void *dev, size_t n)
+{
+  ok(tbg_copy_out(host, dev, n, 0, NULL), "copy out");
+  g_d2h_bytes += n;
+}
+
+enum { PART_W, PART_CAND, PART_VERIFY };
+typedef struct {
+  int kind, stm, n, more, cls;
+  uint64_t after;  /* inbound copies of the part wait for this point (0: none) */
+} Part;
+
+static int seg_lo(int h) { return h * g_seg; }
+static int seg_hi(int h) { return (h + 1) * g_seg < NS ? (h + 1) * g_seg : NS; }
+
+/* Reads of segment h (number q) of part P, into staging set q mod 3. */
+static void prep(const Part *P, int h, int64_t q)
+{
+  const int p = (int)(q % NPAR), stm = P->stm, n = P->n;
+  if (h == 0 && P->after) ok(tbg_copy_in(NULL, NULL, 0, P->after, NULL), "wait");
+  if (q >= 3) ok(tbg_copy_in(NULL, NULL, 0, out_tk[(q - 3) % TK_RING], NULL), "wait");
+  int i = 0;
+  for (int k = seg_lo(h); k < seg_hi(h); k++) {
+    const int j = k - seg_lo(h), s = order[stm][k];
+    if (P->kind == PART_W) {
+      if (n == 1 || n == DRAW_RULE + 1)
+        cin(st_sub[p][j], HSUB(stm ^ 1, n == 1 ? C_LOSS : C_BLOSS, s), g_sub);
+      if (P->more) cin(st_src[p][j], HSL(P_LP, stm ^ 1, s), g_bytes);
+      for (int x = 0; x < ntouch[stm][k]; x++) {
+        const int t = touch[stm][k][x];
+        if (last_use[stm][t] == k) cin(st_win[p][i++], HSL(P_WINS, stm, t), g_bytes);
+      }
+    } else if (P->kind == PART_CAND) {
+      if (n == 1) {
+        cin(st_sub[p][j], HSUB(stm ^ 1, C_WIN, s), g_sub);
+      } else if (n == DRAW_RULE + 1) {
+        cin(st_sub[p][j], HSUB(stm ^ 1, C_CWIN, s), g_sub);
+        cin(st_subt[p][j], HSUB(stm ^ 1, C_WIN, s), g_sub);
+      }
+      if (P->more && n > 1) cin(st_src[p][j], HSL(P_WP, stm ^ 1, s), g_bytes);
+    } else {
+      for (int x = 0; x < ntouch[stm][k]; x++) {
+        const int t = touch[stm][k][x];
+        if (where_[t] >= 0) continue;
+        const int b = take(q - 3);
+        where_[t] = b;
+        cin(win[b].bm, HSL(P_WINS, stm ^ 1, t), g_bytes);
+        cin(win[b].sub, HSUB(stm ^ 1, P->cls, t), g_sub);
+      }
+      cin(st_src[p][j], HSL(P_X, stm, s), g_bytes);
+    }
+  }
+  ok(tbg_copy_in(NULL, NULL, 0, 0, &in_tk[q % TK_RING]), "fence");
+}
+
+/* Kernels and writes of segment h (number q) of part P. */
+static void compute(const Part *P, int h, int64_t q)
+{
+  const int p = (int)(q % NPAR), stm = P->stm, n = P->n;
+  ok(tbg_join(in_tk[q % TK_RING]), "join");
+  if (q >= 2) ok(tbg_join(out_tk[(q - 2) % TK_RING]), "join");
+  if (P->kind == PART_CAND && n == DRAW_RULE + 1) /* cwin \ win (tb8gen.c:964-970) */
+    for (int k = seg_lo(h); k < seg_hi(h); k++) {
+      const int j = k - seg_lo(h);
+      ok(tbg_bitmap_and_not(st_sub[p][j], st_sub[p][j], st_subt[p][j], g_sub), "and_not");
+    }
+  ok(tbg_batch_begin(), "batch begin");
+  int i = 0;
+  for (int k = seg_lo(h); k < seg_hi(h); k++) {
+    const int j = k - seg_lo(h), s = order[stm][k];
+    if (P->kind == PART_VERIFY) {
+      for (int x = 0; x < ntouch[stm][k]; x++) {
+        const int t = touch[stm][k][x];
+        ok(tbg_slot_bind(t, win[where_[t]].bm, g_bytes), "bind");
+        ok(tbg_sub_bind(t, win[where_[t]].sub, g_sub), "bind sub");
+      }
+      ok(tbg_slot_bind(-1, st_src[p][j], g_bytes), "bind");
+      ok(tbg_check_successors(stm, s), "check_successors");
+      ok(tbg_batch_count(-1), "count");
+      continue;
+    }
+    for (int x = 0; x < ntouch[stm][k]; x++) {
+      const int t = touch[stm][k][x];
+      if (where_[t] >= 0) continue;
+      const int b = take(q - 2);
+      where_[t] = b;
+      ok(tbg_slot_bind(t, win[b].bm, g_bytes), "bind");
+      ok(tbg_clear(t), "clear");
+    }
+    if (n == 1 || n == DRAW_RULE + 1) {
+      ok(tbg_sub_bind(s, st_sub[p][j], g_sub), "bind sub");
+      ok(tbg_predecessors_sub(stm, s, P->kind == PART_CAND && n == 1), "predecessors_sub");
+      ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
+    }
+    if (P->kind == PART_W ? P->more : (P->more && n > 1)) {
+      ok(tbg_slot_bind(-1, st_src[p][j], g_bytes), "bind");
+      ok(tbg_predecessors(stm, s), "predecessors");
+    }
+    if (P->kind == PART_W)
+      for (int x = 0; x < ntouch[stm][k]; x++) {
+        const int t = touch[stm][k][x];
+        if (last_use[stm][t] == k)
+          ok(tbg_epilogue_W_to(t, st_win[p][i], st_win[p][i], NULL), "epilogue");
+        i += last_use[stm][t] == k;
+      }
+  }
+  int nops;
+  uint64_t items;
+  ok(tbg_batch_end(&nops, &items), "batch end");
+  ok(tbg_batch_run(1), "batch run");
+  const int nc = P->kind == PART_W ? i : P->kind == PART_VERIFY ? seg_hi(h) - seg_lo(h) : 0;
+  if (nc) ok(tbg_batch_counts_async(hcnt + ncnt, nc), "counts");
+  ncnt += nc;
+  uint64_t mk;
+  ok(tbg_mark(&mk), "mark");
+  ok(tbg_copy_out(NULL, NULL, 0, mk, NULL), "wait");
+  i = 0;
+  for (int k = seg_lo(h); k < seg_hi(h); k++) {
+    const int j = k - seg_lo(h), s = order[stm][k];
+    if (P->kind == PART_VERIFY) {
+      cout_(HSL(P_LC, stm, s), st_src[p][j], g_bytes);
+      continue;
+    }
+    for (int x = 0; x < ntouch[stm][k]; x++) {
+      const int t = touch[stm][k][x];
+      if (last_use[stm][t] != k) continue;
+      if (P->kind == PART_W) {
+        cout_(HSL(P_WC, stm, t), win[where_[t]].bm, g_bytes);
+        cout_(HSL(P_WINS, stm, t), st_win[p][i++], g_bytes);
+      } else {
+        cout_(HSL(P_X, stm, t), win[where_[t]].bm, g_bytes);
+      }
+    }
+  }
+  ok(tbg_copy_out(NULL, NULL, 0, 0, &out_tk[q % TK_RING]), "fence");
+  for (int k = seg_lo(h); k < seg_hi(h); k++)
+    for (int x = 0; x < ntouch[stm][k]; x++) {
+      const int t = touch[stm][k][x];
+      if (last_use[stm][t] == k) release(t, q);
+    }
+}
+
+/* Runs a part; returns the outbound point after its last writes. */
+static uint64_t run_part(const Part *P)
+{
+  const int nseg = (NS + g_seg - 1) / g_seg;
+  const int64_t base = g_seq;
+  g_seq += nseg;
+  if (P->after) reset_window();  /* its reads wait for every earlier write */
+  prep(P, 0, base);
+  for (int h = 0; h < nseg; h++) {
+    if (h + 1 < nseg) prep(P, h + 1, base + h + 1);
+    compute(P, h, base + h);
+  }
+  return out_tk[(base + nseg - 1) % TK_RING];
+}
+
+/* Sum of the counts the half-ply queued, once its last writes are done. */
+static uint64_t half_ply_count(uint64_t last)
+{
+  ok(tbg_wait_ticket(last, 0), "wait");
+  ok(tbg_sync(0), "sync");
+  reset_window();
+  uint64_t cnt = 0;
+  for (int k = 0; k < ncnt; k++) cnt += hcnt[k];
+  ncnt = 0;
+  return cnt;
 }
 
 /* calc_W_n streamed (tb8gen.c:1028-1084). */
 static int st_calc_W_n(int stm, int n, int more_w)
 {
-  uint64_t cnt = 0;
-  for (int k = 0; k < NS; k++) {
-    int s = order[stm][k];
-    for (int j = 0; j < ntouch[stm][k]; j++) enter_target(touch[stm][k][j]);
-    if (n == 1 || n == DRAW_RULE + 1) {
-      h2d(dsub_src, HSUB(stm ^ 1, n == 1 ? C_LOSS : C_BLOSS, s), g_sub);
-      ok(tbg_sub_bind(s, dsub_src, g_sub), "bind sub");
-      ok(tbg_predecessors_sub(stm, s, 0), "predecessors_sub");
-      ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
-    }
-    if (more_w) {
-      h2d(dsrc, HSL(P_LP, stm ^ 1, s), g_bytes);
-      ok(tbg_slot_bind(-1, dsrc, g_bytes), "bind");
-      ok(tbg_predecessors(stm, s), "predecessors");
-    }
-    for (int j = 0; j < ntouch[stm][k]; j++) {
-      int t = touch[stm][k][j];
-      if (last_use[stm][t] != k) continue;
-      h2d(dwins, HSL(P_WINS, stm, t), g_bytes);
-      ok(tbg_epilogue_W_to(t, dwins, dwins, NULL), "epilogue");
-      d2h(HSL(P_WC, stm, t), wbuf[where_[t]], g_bytes);
-      d2h(HSL(P_WINS, stm, t), dwins, g_bytes);
-      leave(t);
-    }
-  }
-  cnt = plane_count(HP[stm][P_WC]);
+  Part P = { PART_W, stm, n, more_w, 0, 0 };
+  uint64_t cnt = half_ply_count(run_part(&P));
   printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
   return cnt != 0;
 }
@@ -453,59 +675,10 @@ static int st_calc_W_n(int stm, int n, int more_w)
  * plane, then the verify. */
 static int st_calc_L_n(int stm, int n, int more_l)
 {
-  uint64_t cnt = 0;
-  for (int k = 0; k < NS; k++) {
-    int s = order[stm][k];
-    for (int j = 0; j < ntouch[stm][k]; j++) enter_target(touch[stm][k][j]);
-    if (n == 1) {
-      h2d(dsub_src, HSUB(stm ^ 1, C_WIN, s), g_sub);
-      ok(tbg_sub_bind(s, dsub_src, g_sub), "bind sub");
-      ok(tbg_predecessors_sub(stm, s, 1), "predecessors_sub");
-      ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
-    } else if (n == DRAW_RULE + 1) {
-      /* cwin \ win (tb8gen.c:964-970) */
-      h2d(dsub_src, HSUB(stm ^ 1, C_CWIN, s), g_sub);
-      h2d(dsub_tmp, HSUB(stm ^ 1, C_WIN, s), g_sub);
-      ok(tbg_bitmap_and_not(dsub_src, dsub_src, dsub_tmp, g_sub), "and_not");
-      ok(tbg_sub_bind(s, dsub_src, g_sub), "bind sub");
-      ok(tbg_predecessors_sub(stm, s, 0), "predecessors_sub");
-      ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
-    }
-    if (more_l && n > 1) {
-      h2d(dsrc, HSL(P_WP, stm ^ 1, s), g_bytes);
-      ok(tbg_slot_bind(-1, dsrc, g_bytes), "bind");
-      ok(tbg_predecessors(stm, s), "predecessors");
-    }
-    for (int j = 0; j < ntouch[stm][k]; j++) {
-      int t = touch[stm][k][j];
-      if (last_use[stm][t] != k) continue;
-      d2h(HSL(P_X, stm, t), wbuf[where_[t]], g_bytes);
-      leave(t);
-    }
-  }
-  int cls = n <= DRAW_RULE ? C_WIN : C_CWIN;
-  for (int k = 0; k < NS; k++) {
-    int s = order[stm][k];
-    for (int j = 0; j < ntouch[stm][k]; j++) {
-      int t = touch[stm][k][j];
-      if (where_[t] >= 0) continue;
-      int b = take();
-      where_[t] = b;
-      h2d(wbuf[b], HSL(P_WINS, stm ^ 1, t), g_bytes);
-      h2d(wsub[b], HSUB(stm ^ 1, cls, t), g_sub);
-      ok(tbg_slot_bind(t, wbuf[b], g_bytes), "bind");
-      ok(tbg_sub_bind(t, wsub[b], g_sub), "bind sub");
-    }
-    h2d(dsrc, HSL(P_X, stm, s), g_bytes);
-    ok(tbg_slot_bind(-1, dsrc, g_bytes), "bind");
-    ok(tbg_check_successors(stm, s), "check_successors");
-    d2h(HSL(P_LC, stm, s), dsrc, g_bytes);
-    for (int j = 0; j < ntouch[stm][k]; j++) {
-      int t = touch[stm][k][j];
-      if (last_use[stm][t] == k) leave(t);
-    }
-  }
-  cnt = plane_count(HP[stm][P_LC]);
+  Part P = { PART_CAND, stm, n, more_l, 0, 0 };
+  uint64_t done = run_part(&P);
+  Part V = { PART_VERIFY, stm, n, more_l, n <= DRAW_RULE ? C_WIN : C_CWIN, done };
+  uint64_t cnt = half_ply_count(run_part(&V));
   printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
   return cnt != 0;
 }
@@ -523,40 +696,59 @@ static void *host_alloc(size_t n)
   return p;
 }
 
-/* Sets up the streamed mode: host planes and the device window. */
+/* Sets up the streamed mode: host planes, the set-up buffers and the
+ * staging sets of the pipeline (the window grows as it needs). */
 static void st_setup(void)
 {
+  if (g_seg == 0) g_seg = g_bytes <= (16u << 20) ? 32 : 8;
   init_king_tables();
   init_schedule();
-  int nbuf = window_max > 5 ? window_max : 5;
   for (int c = 0; c < 2; c++) {
     for (int p = 0; p < NPLANE; p++) HP[c][p] = host_alloc((size_t)g_bytes * NS);
     for (int k = 0; k < 5; k++) HS[c][k] = host_alloc((size_t)g_sub * NS);
   }
-  size_t total = (size_t)g_bytes * (nbuf + 2) + (size_t)g_sub * (nbuf + 2);
-  uint8_t *base;
-  ok(tbg_alloc(total, (void **)&base), "alloc");
-  wbuf = calloc(nbuf, sizeof *wbuf);
-  wsub = calloc(nbuf, sizeof *wsub);
-  wfree = calloc(nbuf, sizeof *wfree);
-  for (int b = 0; b < nbuf; b++) {
-    wbuf[b] = base;
-    base += g_bytes;
-    wsub[b] = base;
-    base += g_sub;
-    wfree[nfree++] = nbuf - 1 - b;
+  hcnt = host_alloc(NS * sizeof *hcnt);
+  for (int stm = 0; stm < 2; stm++)
+    for (int h = 0; h * g_seg < NS; h++) {
+      int lw = 0;
+      for (int k = seg_lo(h); k < seg_hi(h); k++)
+        for (int x = 0; x < ntouch[stm][k]; x++) lw += last_use[stm][touch[stm][k][x]] == k;
+      if (lw > g_lw) g_lw = lw;
+    }
+  ok(tbg_alloc(4 * g_bytes + 5 * g_sub, (void **)&setup_base), "alloc");
+  for (int j = 0; j < 4; j++) setup_bm[j] = setup_base + j * g_bytes;
+  for (int k = 0; k < 5; k++) setup_sub[k] = setup_base + 4 * g_bytes + k * g_sub;
+  const size_t per_set = (size_t)g_seg * (g_bytes + 2 * g_sub) + (size_t)g_lw * g_bytes;
+  for (int p = 0; p < NPAR; p++) {
+    uint8_t *base;
+    ok(tbg_alloc(per_set, (void **)&base), "alloc");
+    for (int j = 0; j < g_seg; j++) {
+      st_src[p][j] = base;
+      base += g_bytes;
+      st_sub[p][j] = base;
+      base += g_sub;
+      st_subt[p][j] = base;
+      base += g_sub;
+    }
+    st_win[p] = calloc(g_lw, sizeof *st_win[p]);
+    for (int i = 0; i < g_lw; i++) {
+      st_win[p][i] = base;
+      base += g_bytes;
+    }
   }
-  dsrc = base;
-  base += g_bytes;
-  dwins = base;
-  base += g_bytes;
-  dsub_src = base;
-  base += g_sub;
-  dsub_tmp = base;
   for (int s = 0; s < NS; s++) where_[s] = -1;
   if (!quiet)
-    fprintf(stderr, "tbgen: streamed, window of %d slices, host tier %.1f GB\n", nbuf,
-            (double)(NPLANE * g_bytes + 5 * g_sub) * NS * 2 / 1e9);
+    fprintf(stderr,
+            "tbgen: streamed, segments of %d steps, schedule window %d slices, host tier %.1f GB\n",
+            g_seg, window_max, (double)(NPLANE * g_bytes + 5 * g_sub) * NS * 2 / 1e9);
+}
+
+/* After the set-up steps (copies on the library stream): the host tier is
+ * complete before the pipeline's streams read it. */
+static void st_setup_done(void)
+{
+  ok(tbg_sync(0), "sync");
+  ok(tbg_free(setup_base), "free");
 }
 
 static void swap_host_planes(void)
@@ -592,18 +784,25 @@ int main(int argc, char **argv)
   uint64_t seed = 1;
   int mod = 3, opt, force_stream = 0, max_ply = 1 << 30;
   double budget_mb = 0;
-  while ((opt = getopt(argc, argv, "s:m:qb:Spn:")) != -1) {
+  while ((opt = getopt(argc, argv, "s:m:qb:SPpn:g:")) != -1) {
     if (opt == 's') seed = strtoull(optarg, NULL, 10);
     else if (opt == 'm') mod = atoi(optarg);
     else if (opt == 'q') quiet = 1;
     else if (opt == 'b') budget_mb = atof(optarg);
     else if (opt == 'S') force_stream = 1;
+    else if (opt == 'P') g_plain = 1;
     else if (opt == 'p') g_timing = 1;
     else if (opt == 'n') max_ply = atoi(optarg);
+    else if (opt == 'g') g_seg = atoi(optarg);
   }
   if (optind >= argc) {
     fprintf(stderr,
-            "usage: tbgen [-s seed] [-m 3|5] [-b device_MB] [-S] [-p] [-n max_ply] MATERIAL\n");
+            "usage: tbgen [-s seed] [-m 3|5] [-b device_MB] [-S] [-g steps] [-P] [-p] [-n max_ply] "
+            "MATERIAL\n");
+    return EXIT_FAILURE;
+  }
+  if (g_seg < 0 || g_seg > MAX_SEG) {
+    fprintf(stderr, "tbgen: -g takes 1..%d steps per segment (0: automatic)\n", MAX_SEG);
     return EXIT_FAILURE;
   }
   ok(tbg_init(), "init");
@@ -622,6 +821,7 @@ int main(int argc, char **argv)
     st_setup();
     st_calc_subs();
     st_illegal_and_mate();
+    st_setup_done();
     W = st_calc_W_n;
     L = st_calc_L_n;
   } else {

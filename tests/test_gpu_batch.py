@@ -78,3 +78,21 @@ def test_batch_matches_reference(setup):
         assert np.array_equal(T, cpu.T), f"W of {j.material} slice {j.s}"
         assert np.array_equal(W, cpu.wins), f"wins of {j.material} slice {j.s}"
         assert np.array_equal(X, cpu.X), f"L of {j.material} slice {j.s}"
+
+
+def test_count_strided(setup):
+    """tbg_count_strided: ones below the slice size in each of n bitmaps at a
+    fixed stride (bits past the size and the gaps between bitmaps are not
+    counted), equal to numpy's count."""
+    torch, tbg, jobs, pools, nops = setup
+    m = tbg.Material("KRRvKR").select()
+    rng = np.random.default_rng(5)
+    for n, gap in ((1, 0), (7, 0), (462, 48)):
+        stride = m.bytes + gap
+        host = rng.integers(0, 256, size=n * stride, dtype=np.uint8)
+        dev = torch.from_numpy(host).cuda()
+        want = 0
+        for i in range(n):
+            bits = np.unpackbits(host[i * stride:i * stride + m.bytes], bitorder="little")
+            want += int(bits[:m.size].sum())
+        assert tbg.count_strided(dev, stride, n) == want

@@ -6,7 +6,10 @@ material (tests/golden/schedule_counts.json, made by
 tests/golden/make_schedule_golden.py).  KRvK and KQvK are the reference's
 real results (captures into KvK are draws); the others replace the 7-piece
 probe by the seeded stub on both sides.  KRvKN uses the five-valued stub, so
-cursed wins and blessed losses reach the ply-101 paths."""
+cursed wins and blessed losses reach the ply-101 paths.  The resident
+driver runs each half-ply as one recorded batch (the persistent kernel);
+with -P it launches every call on its own: both must print the golden
+counts."""
 import json
 import os
 import subprocess
@@ -23,13 +26,14 @@ with open(GOLDEN) as f:
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("path", ["batched", "plain"])
 @pytest.mark.parametrize("material", sorted(CASES))
-def test_generation_counts_match_reference(material):
+def test_generation_counts_match_reference(material, path):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     case = CASES[material]
-    cmd = [TBGEN]
+    cmd = [TBGEN] + (["-P"] if path == "plain" else [])
     if case["seed"] is not None:
         cmd += ["-s", str(case["seed"]), "-m", str(case["mod"])]
     r = subprocess.run(cmd + [material], capture_output=True, text=True, timeout=600)
@@ -38,18 +42,21 @@ def test_generation_counts_match_reference(material):
     assert got == case["lines"]
 
 
-STREAMED = ["KRvK", "KRRvK", "KRvKN", "KRRvKR"]
+STREAMED = [("KRvK", 16), ("KRRvK", 16), ("KRvKN", 16), ("KRRvKR", 16), ("KRvKN", 1),
+            ("KRRvKR", 5), ("KQvKR", 64)]
 
 
-@pytest.mark.parametrize("material", STREAMED)
-def test_streamed_generation_counts_match_reference(material):
+@pytest.mark.parametrize("material,seg", STREAMED)
+def test_streamed_generation_counts_match_reference(material, seg):
     """The same generations with the planes in host memory and a device
-    window of slices that follows the schedule (tbgen -S): identical counts."""
+    window of slices that follows the schedule (tbgen -S), its steps run in
+    pipelined segments of `seg` steps (reads, kernels and writes of adjacent
+    segments overlap on three streams): identical counts."""
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     case = CASES[material]
-    cmd = [TBGEN, "-S"]
+    cmd = [TBGEN, "-S", "-g", str(seg)]
     if case["seed"] is not None:
         cmd += ["-s", str(case["seed"]), "-m", str(case["mod"])]
     r = subprocess.run(cmd + [material], capture_output=True, text=True, timeout=900)
