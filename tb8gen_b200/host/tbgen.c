@@ -379,6 +379,13 @@ static uint8_t *HP[2][NPLANE], *HS[2][5];
 #define HSL(plane, c, s) (HP[c][plane] + (size_t)(s) * g_bytes)
 #define HSUB(c, k, s) (HS[c][k] + (size_t)(s) * g_sub)
 
+/* Slices of a host-tier plane known to hold no position (from the counts of
+ * the step that wrote them): their bytes are not kept and never read.  An
+ * empty source is neither copied nor scattered; a slice that no scatter
+ * reaches stays empty, so it is neither cleared, nor finished by an
+ * epilogue, nor written back; a verify step with no candidates is skipped. */
+static uint8_t hempty[2][NPLANE][NS];
+
 /* device buffers of the set-up steps (calc_sub, illegal and mate) */
 static uint8_t *setup_bm[4], *setup_sub[5], *setup_base;
 
@@ -403,6 +410,7 @@ static void st_illegal_and_mate(void)
       ok(tbg_slot_bind(0, b[j], g_bytes), "bind");
       ok(tbg_count(0, &c), "count");
       cnt[j] += c;
+      if (j >= 2) hempty[j - 2][P_LP][s] = c == 0;
     }
     ok(tbg_slot_bind(0, NULL, 0), "unbind");
     d2h(HSL(P_WINS, WHITE, s), b[0], g_bytes);
@@ -508,6 +516,34 @@ typedef struct {
 static int seg_lo(int h) { return h * g_seg; }
 static int seg_hi(int h) { return (h + 1) * g_seg < NS ? (h + 1) * g_seg : NS; }
 
+static uint8_t act[NS];      /* schedule step k of the current part has work */
+static uint8_t hit[NS];      /* slice t is marked (scatters) or read (verify) */
+static int cnt_slice[NS];    /* slice of each count queued in the half-ply */
+
+static int has_sub(const Part *P)
+{
+  return P->kind != PART_VERIFY && (P->n == 1 || P->n == DRAW_RULE + 1);
+}
+
+static int has_src(const Part *P, int s)
+{
+  if (P->kind == PART_W) return P->more && !hempty[P->stm ^ 1][P_LP][s];
+  if (P->kind == PART_CAND) return P->more && P->n > 1 && !hempty[P->stm ^ 1][P_WP][s];
+  return 0;
+}
+
+static void plan_part(const Part *P)
+{
+  const int stm = P->stm;
+  memset(hit, 0, sizeof hit);
+  for (int k = 0; k < NS; k++) {
+    const int s = order[stm][k];
+    act[k] = P->kind == PART_VERIFY ? !hempty[stm][P_X][s] : has_sub(P) || has_src(P, s);
+    if (act[k])
+      for (int x = 0; x < ntouch[stm][k]; x++) hit[touch[stm][k][x]] = 1;
+  }
+}
+
 /* Reads of segment h (number q) of part P, into staging set q mod 3. */
 static void prep(const Part *P, int h, int64_t q)
 {
@@ -517,23 +553,8 @@ static void prep(const Part *P, int h, int64_t q)
   int i = 0;
   for (int k = seg_lo(h); k < seg_hi(h); k++) {
     const int j = k - seg_lo(h), s = order[stm][k];
-    if (P->kind == PART_W) {
-      if (n == 1 || n == DRAW_RULE + 1)
-        cin(st_sub[p][j], HSUB(stm ^ 1, n == 1 ? C_LOSS : C_BLOSS, s), g_sub);
-      if (P->more) cin(st_src[p][j], HSL(P_LP, stm ^ 1, s), g_bytes);
-      for (int x = 0; x < ntouch[stm][k]; x++) {
-        const int t = touch[stm][k][x];
-        if (last_use[stm][t] == k) cin(st_win[p][i++], HSL(P_WINS, stm, t), g_bytes);
-      }
-    } else if (P->kind == PART_CAND) {
-      if (n == 1) {
-        cin(st_sub[p][j], HSUB(stm ^ 1, C_WIN, s), g_sub);
-      } else if (n == DRAW_RULE + 1) {
-        cin(st_sub[p][j], HSUB(stm ^ 1, C_CWIN, s), g_sub);
-        cin(st_subt[p][j], HSUB(stm ^ 1, C_WIN, s), g_sub);
-      }
-      if (P->more && n > 1) cin(st_src[p][j], HSL(P_WP, stm ^ 1, s), g_bytes);
-    } else {
+    if (P->kind == PART_VERIFY) {
+      if (!act[k]) continue;
       for (int x = 0; x < ntouch[stm][k]; x++) {
         const int t = touch[stm][k][x];
         if (where_[t] >= 0) continue;
@@ -543,9 +564,35 @@ static void prep(const Part *P, int h, int64_t q)
         cin(win[b].sub, HSUB(stm ^ 1, P->cls, t), g_sub);
       }
       cin(st_src[p][j], HSL(P_X, stm, s), g_bytes);
+      continue;
     }
+    if (has_sub(P)) {
+      if (P->kind == PART_W) {
+        cin(st_sub[p][j], HSUB(stm ^ 1, n == 1 ? C_LOSS : C_BLOSS, s), g_sub);
+      } else if (n == 1) {
+        cin(st_sub[p][j], HSUB(stm ^ 1, C_WIN, s), g_sub);
+      } else {
+        cin(st_sub[p][j], HSUB(stm ^ 1, C_CWIN, s), g_sub);
+        cin(st_subt[p][j], HSUB(stm ^ 1, C_WIN, s), g_sub);
+      }
+    }
+    if (has_src(P, s))
+      cin(st_src[p][j], HSL(P->kind == PART_W ? P_LP : P_WP, stm ^ 1, s), g_bytes);
+    if (P->kind == PART_W)
+      for (int x = 0; x < ntouch[stm][k]; x++) {
+        const int t = touch[stm][k][x];
+        if (last_use[stm][t] == k && hit[t]) cin(st_win[p][i++], HSL(P_WINS, stm, t), g_bytes);
+      }
   }
   ok(tbg_copy_in(NULL, NULL, 0, 0, &in_tk[q % TK_RING]), "fence");
+}
+
+static int g_recording;
+
+static void rec(void)
+{
+  if (!g_recording) ok(tbg_batch_begin(), "batch begin");
+  g_recording = 1;
 }
 
 /* Kernels and writes of segment h (number q) of part P. */
@@ -559,11 +606,12 @@ static void compute(const Part *P, int h, int64_t q)
       const int j = k - seg_lo(h);
       ok(tbg_bitmap_and_not(st_sub[p][j], st_sub[p][j], st_subt[p][j], g_sub), "and_not");
     }
-  ok(tbg_batch_begin(), "batch begin");
-  int i = 0;
+  int i = 0, nc = 0;
   for (int k = seg_lo(h); k < seg_hi(h); k++) {
     const int j = k - seg_lo(h), s = order[stm][k];
     if (P->kind == PART_VERIFY) {
+      if (!act[k]) continue;
+      rec();
       for (int x = 0; x < ntouch[stm][k]; x++) {
         const int t = touch[stm][k][x];
         ok(tbg_slot_bind(t, win[where_[t]].bm, g_bytes), "bind");
@@ -572,39 +620,47 @@ static void compute(const Part *P, int h, int64_t q)
       ok(tbg_slot_bind(-1, st_src[p][j], g_bytes), "bind");
       ok(tbg_check_successors(stm, s), "check_successors");
       ok(tbg_batch_count(-1), "count");
+      cnt_slice[ncnt + nc++] = s;
       continue;
     }
-    for (int x = 0; x < ntouch[stm][k]; x++) {
-      const int t = touch[stm][k][x];
-      if (where_[t] >= 0) continue;
-      const int b = take(q - 2);
-      where_[t] = b;
-      ok(tbg_slot_bind(t, win[b].bm, g_bytes), "bind");
-      ok(tbg_clear(t), "clear");
-    }
-    if (n == 1 || n == DRAW_RULE + 1) {
-      ok(tbg_sub_bind(s, st_sub[p][j], g_sub), "bind sub");
-      ok(tbg_predecessors_sub(stm, s, P->kind == PART_CAND && n == 1), "predecessors_sub");
-      ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
-    }
-    if (P->kind == PART_W ? P->more : (P->more && n > 1)) {
-      ok(tbg_slot_bind(-1, st_src[p][j], g_bytes), "bind");
-      ok(tbg_predecessors(stm, s), "predecessors");
+    if (act[k]) {
+      rec();
+      for (int x = 0; x < ntouch[stm][k]; x++) {
+        const int t = touch[stm][k][x];
+        if (where_[t] >= 0) continue;
+        const int b = take(q - 2);
+        where_[t] = b;
+        ok(tbg_slot_bind(t, win[b].bm, g_bytes), "bind");
+        ok(tbg_clear(t), "clear");
+      }
+      if (has_sub(P)) {
+        ok(tbg_sub_bind(s, st_sub[p][j], g_sub), "bind sub");
+        ok(tbg_predecessors_sub(stm, s, P->kind == PART_CAND && n == 1), "predecessors_sub");
+        ok(tbg_sub_bind(s, NULL, 0), "unbind sub");
+      }
+      if (has_src(P, s)) {
+        ok(tbg_slot_bind(-1, st_src[p][j], g_bytes), "bind");
+        ok(tbg_predecessors(stm, s), "predecessors");
+      }
     }
     if (P->kind == PART_W)
       for (int x = 0; x < ntouch[stm][k]; x++) {
         const int t = touch[stm][k][x];
-        if (last_use[stm][t] == k)
-          ok(tbg_epilogue_W_to(t, st_win[p][i], st_win[p][i], NULL), "epilogue");
-        i += last_use[stm][t] == k;
+        if (last_use[stm][t] != k || !hit[t]) continue;
+        rec();
+        ok(tbg_epilogue_W_to(t, st_win[p][i], st_win[p][i], NULL), "epilogue");
+        cnt_slice[ncnt + nc++] = t;
+        i++;
       }
   }
-  int nops;
-  uint64_t items;
-  ok(tbg_batch_end(&nops, &items), "batch end");
-  ok(tbg_batch_run(1), "batch run");
-  const int nc = P->kind == PART_W ? i : P->kind == PART_VERIFY ? seg_hi(h) - seg_lo(h) : 0;
-  if (nc) ok(tbg_batch_counts_async(hcnt + ncnt, nc), "counts");
+  if (g_recording) {
+    int nops;
+    uint64_t items;
+    ok(tbg_batch_end(&nops, &items), "batch end");
+    ok(tbg_batch_run(1), "batch run");
+    if (nc) ok(tbg_batch_counts_async(hcnt + ncnt, nc), "counts");
+    g_recording = 0;
+  }
   ncnt += nc;
   uint64_t mk;
   ok(tbg_mark(&mk), "mark");
@@ -613,17 +669,23 @@ static void compute(const Part *P, int h, int64_t q)
   for (int k = seg_lo(h); k < seg_hi(h); k++) {
     const int j = k - seg_lo(h), s = order[stm][k];
     if (P->kind == PART_VERIFY) {
-      cout_(HSL(P_LC, stm, s), st_src[p][j], g_bytes);
+      if (act[k]) cout_(HSL(P_LC, stm, s), st_src[p][j], g_bytes);
+      else hempty[stm][P_LC][s] = 1;
       continue;
     }
     for (int x = 0; x < ntouch[stm][k]; x++) {
       const int t = touch[stm][k][x];
       if (last_use[stm][t] != k) continue;
       if (P->kind == PART_W) {
-        cout_(HSL(P_WC, stm, t), win[where_[t]].bm, g_bytes);
-        cout_(HSL(P_WINS, stm, t), st_win[p][i++], g_bytes);
+        if (hit[t]) {
+          cout_(HSL(P_WC, stm, t), win[where_[t]].bm, g_bytes);
+          cout_(HSL(P_WINS, stm, t), st_win[p][i++], g_bytes);
+        } else {
+          hempty[stm][P_WC][t] = 1;
+        }
       } else {
-        cout_(HSL(P_X, stm, t), win[where_[t]].bm, g_bytes);
+        if (hit[t]) cout_(HSL(P_X, stm, t), win[where_[t]].bm, g_bytes);
+        hempty[stm][P_X][t] = !hit[t];
       }
     }
   }
@@ -631,7 +693,7 @@ static void compute(const Part *P, int h, int64_t q)
   for (int k = seg_lo(h); k < seg_hi(h); k++)
     for (int x = 0; x < ntouch[stm][k]; x++) {
       const int t = touch[stm][k][x];
-      if (last_use[stm][t] == k) release(t, q);
+      if (last_use[stm][t] == k && where_[t] >= 0) release(t, q);
     }
 }
 
@@ -641,6 +703,7 @@ static uint64_t run_part(const Part *P)
   const int nseg = (NS + g_seg - 1) / g_seg;
   const int64_t base = g_seq;
   g_seq += nseg;
+  plan_part(P);
   if (P->after) reset_window();  /* its reads wait for every earlier write */
   prep(P, 0, base);
   for (int h = 0; h < nseg; h++) {
@@ -650,14 +713,18 @@ static uint64_t run_part(const Part *P)
   return out_tk[(base + nseg - 1) % TK_RING];
 }
 
-/* Sum of the counts the half-ply queued, once its last writes are done. */
-static uint64_t half_ply_count(uint64_t last)
+/* Sum of the counts the half-ply queued, once its last writes are done;
+ * a slice whose count is 0 is flagged empty in `plane`. */
+static uint64_t half_ply_count(uint64_t last, int stm, int plane)
 {
   ok(tbg_wait_ticket(last, 0), "wait");
   ok(tbg_sync(0), "sync");
   reset_window();
   uint64_t cnt = 0;
-  for (int k = 0; k < ncnt; k++) cnt += hcnt[k];
+  for (int k = 0; k < ncnt; k++) {
+    cnt += hcnt[k];
+    hempty[stm][plane][cnt_slice[k]] = hcnt[k] == 0;
+  }
   ncnt = 0;
   return cnt;
 }
@@ -666,7 +733,7 @@ static uint64_t half_ply_count(uint64_t last)
 static int st_calc_W_n(int stm, int n, int more_w)
 {
   Part P = { PART_W, stm, n, more_w, 0, 0 };
-  uint64_t cnt = half_ply_count(run_part(&P));
+  uint64_t cnt = half_ply_count(run_part(&P), stm, P_WC);
   printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
   return cnt != 0;
 }
@@ -678,7 +745,7 @@ static int st_calc_L_n(int stm, int n, int more_l)
   Part P = { PART_CAND, stm, n, more_l, 0, 0 };
   uint64_t done = run_part(&P);
   Part V = { PART_VERIFY, stm, n, more_l, n <= DRAW_RULE ? C_WIN : C_CWIN, done };
-  uint64_t cnt = half_ply_count(run_part(&V));
+  uint64_t cnt = half_ply_count(run_part(&V), stm, P_LC);
   printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
   return cnt != 0;
 }
@@ -754,6 +821,14 @@ static void st_setup_done(void)
 static void swap_host_planes(void)
 {
   for (int c = 0; c < 2; c++) {
+    for (int s = 0; s < NS; s++) {
+      uint8_t e = hempty[c][P_WP][s];
+      hempty[c][P_WP][s] = hempty[c][P_WC][s];
+      hempty[c][P_WC][s] = e;
+      e = hempty[c][P_LP][s];
+      hempty[c][P_LP][s] = hempty[c][P_LC][s];
+      hempty[c][P_LC][s] = e;
+    }
     uint8_t *t = HP[c][P_WP];
     HP[c][P_WP] = HP[c][P_WC];
     HP[c][P_WC] = t;
