@@ -357,46 +357,97 @@ def run_engine(a, rank, world, local):
 
 
 def run_e2e(a, jobs, stream, positions, mode):
-    """Same steps through the C ABI with the sources in pinned host memory:
-    per step H2D of L_prev and W_prev of every slice, the ply (the "wins"
-    bitmaps stay resident in HBM, as the tables of a generation do), and D2H
-    of the results W(s) and L(s)."""
+    """Same steps through the C ABI with the inputs in pinned host memory:
+    per step the H2D copy of L_prev and W_prev of every slice, the ply (the
+    "wins" bitmaps stay resident in HBM, as the tables of a generation do)
+    and the D2H copy of the results W(s) and L(s).  Steps alternate between
+    two device buffer sets, each recorded in its own batch slot, so that
+    step i+1's inputs go in and step i's results come out on the library's
+    copy streams (ordered by tickets) while the kernels of the step between
+    them run.  The host results of the last step are checked against the
+    device buffers."""
     import torch
 
     import tb8gen_b200 as tbg
+    from tb8gen_b200.plyjob import record_step
 
-    host_in, host_out = [], []
+    names = ("L_prev", "W_prev", "T", "X")
+    sets = [[tuple(getattr(j, n) for n in names) for j in jobs]]
+    sets.append([(j.L_prev.clone(), j.W_prev.clone(), torch.zeros_like(j.T), torch.zeros_like(j.X))
+                 for j in jobs])
+    # the second set's step, recorded in batch slot 1
+    for j, bufs in zip(jobs, sets[1]):
+        for n, t in zip(names, bufs):
+            setattr(j, n, t)
+    tbg.batch_select(1)
+    try:
+        record_step(jobs)
+    finally:
+        tbg.batch_select(0)
+        for j, bufs in zip(jobs, sets[0]):
+            for n, t in zip(names, bufs):
+                setattr(j, n, t)
+    pin = lambda t: torch.empty(t.numel(), dtype=torch.uint8, pin_memory=True)
+    host_in = []
     for j in jobs:
-        hi = [torch.empty(j.B, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+        hi = [pin(j.L_prev), pin(j.W_prev)]
         hi[0].copy_(j.L_prev)
         hi[1].copy_(j.W_prev)
         host_in.append(hi)
-        host_out.append([torch.empty(j.B, dtype=torch.uint8, pin_memory=True) for _ in range(2)])
+    host_out = [[(pin(j.T), pin(j.X)) for j in jobs] for _ in range(2)]
     torch.cuda.synchronize()
     h2d = sum(j.B * 2 for j in jobs)
-    steps = max(2, min(a.steps, 5))
 
-    def one():
-        for j, hi in zip(jobs, host_in):
-            j.L_prev.copy_(hi[0], non_blocking=True)
-            j.W_prev.copy_(hi[1], non_blocking=True)
-        tbg.batch_run(mode)
-        for j, ho in zip(jobs, host_out):
-            ho[0].copy_(j.T, non_blocking=True)
-            ho[1].copy_(j.X, non_blocking=True)
+    def run(nsteps):
+        start = tbg.mark()
+        in_t, mk, out_t = {}, {}, {}
 
-    one()
+        def put(i):
+            b = i % 2
+            after = mk[i - 2] if i >= 2 else start  # set b last read by step i-2
+            t = 0
+            for k, (hi, bufs) in enumerate(zip(host_in, sets[b])):
+                tbg.copy_in(bufs[0], hi[0], after if k == 0 else 0)
+                t = tbg.copy_in(bufs[1], hi[1], ticket=True)
+            in_t[i] = t
+
+        put(0)
+        for i in range(nsteps):
+            b = i % 2
+            if i + 1 < nsteps:
+                put(i + 1)
+            tbg.join(in_t[i])
+            if i >= 2:
+                tbg.join(out_t[i - 2])  # set b's results of step i-2 are out
+            tbg.batch_select(b)
+            tbg.batch_run(mode)
+            mk[i] = tbg.mark()
+            t = 0
+            for k, (ho, bufs) in enumerate(zip(host_out[b], sets[b])):
+                tbg.copy_out(ho[0], bufs[2], mk[i] if k == 0 else 0)
+                t = tbg.copy_out(ho[1], bufs[3], ticket=True)
+            out_t[i] = t
+        tbg.join(out_t[nsteps - 1])
+        tbg.batch_select(0)
+        return (nsteps - 1) % 2
+
+    run(2)
     torch.cuda.synchronize()
+    steps = max(2, min(a.steps, 5))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(steps):
-        one()
+    last = run(steps)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    for ho, bufs in zip(host_out[last], sets[last]):
+        assert torch.equal(ho[0], bufs[2].cpu()) and torch.equal(ho[1], bufs[3].cpu()), \
+            "host results differ from the device's"
     return {"value": round(positions / (ms / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms, 3),
-            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "steps": steps}
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "steps": steps,
+            "pipeline": "two buffer sets in two batch slots; copies on the library's copy "
+                        "streams overlap the other set's kernels"}
 
 
 def cpu_oracle(material, nthreads):
@@ -756,35 +807,72 @@ def run_probe(a, rank, world, local):
 
 def run_probe_e2e(a, ps, stream):
     """Probe batches through the C ABI from pinned host memory: per step the
-    H2D copy of every query and the D2H copy of every result."""
+    H2D copy of every query and the D2H copy of every result.  Steps
+    alternate between two device sets of queries and results, so that step
+    i+1's queries go in and step i's results come out on the library's copy
+    streams while the probes between them run.  The host results of the last
+    step are checked against the device's."""
     import torch
 
+    import tb8gen_b200 as tbg
+
     hq = [torch.empty(q.numel(), dtype=torch.uint8, pin_memory=True) for _, _, q, _ in ps.items]
-    ho = [torch.empty(o.numel(), dtype=torch.int8, pin_memory=True) for _, _, _, o in ps.items]
     for h, (_, _, q, _) in zip(hq, ps.items):
         h.copy_(q)
+    sets = [[(q, out) for _, _, q, out in ps.items],
+            [(torch.empty_like(q), torch.empty_like(out)) for _, _, q, out in ps.items]]
+    ho = [[torch.empty(o.numel(), dtype=torch.int8, pin_memory=True) for _, o in sets[0]]
+          for _ in range(2)]
+    tables = [t for _, t, _, _ in ps.items]
     torch.cuda.synchronize()
 
-    def one():
-        for h, r, (_, t, q, out) in zip(hq, ho, ps.items):
-            q.copy_(h, non_blocking=True)
-            t.probe(q, out, 0)
-            r.copy_(out, non_blocking=True)
+    def run(nsteps):
+        start = tbg.mark()
+        in_t, mk, out_t = {}, {}, {}
 
-    one()
+        def put(i):
+            b = i % 2
+            after = mk[i - 2] if i >= 2 else start  # set b's queries last read by step i-2
+            t = 0
+            for k, (h, (q, _)) in enumerate(zip(hq, sets[b])):
+                t = tbg.copy_in(q, h, after if k == 0 else 0, ticket=True)
+            in_t[i] = t
+
+        put(0)
+        for i in range(nsteps):
+            b = i % 2
+            if i + 1 < nsteps:
+                put(i + 1)
+            tbg.join(in_t[i])
+            if i >= 2:
+                tbg.join(out_t[i - 2])  # set b's results of step i-2 are out
+            for t, (q, out) in zip(tables, sets[b]):
+                t.probe(q, out, 0)
+            mk[i] = tbg.mark()
+            t = 0
+            for k, (r, (_, out)) in enumerate(zip(ho[b], sets[b])):
+                t = tbg.copy_out(r, out, mk[i] if k == 0 else 0, ticket=True)
+            out_t[i] = t
+        tbg.join(out_t[nsteps - 1])
+        return (nsteps - 1) % 2
+
+    run(2)
     torch.cuda.synchronize()
     steps = max(2, min(a.steps, 5))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(steps):
-        one()
+    last = run(steps)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    for r, (_, out) in zip(ho[last], sets[last]):
+        assert torch.equal(r, out.cpu()), "host results differ from the device's"
     return {"value": round(ps.positions / (ms / 1e3), 1), "unit": "positions/s",
             "ms_per_step": round(ms, 3), "h2d_bytes_per_step": sum(h.numel() for h in hq),
-            "d2h_bytes_per_step": sum(r.numel() for r in ho), "steps": steps}
+            "d2h_bytes_per_step": sum(r.numel() for r in ho[0]), "steps": steps,
+            "pipeline": "two query/result sets; copies on the library's copy streams "
+                        "overlap the other set's probes"}
 
 
 def run_probe_reference(a, rank, world, local):

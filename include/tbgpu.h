@@ -269,8 +269,16 @@ int tbg_batch_count(int s);
  * ticket marked after it). */
 int tbg_batch_counts_async(uint64_t *host_out, int n);
 
-/* Persistent-launch configuration: CTAs per SM (default 4), and the
- * iteration bound of a dependency wait (<= 0 keeps the current one). */
+/* Selects one of 4 batch slots (default 0); tbg_batch_begin .. counts act
+ * on the selected slot, and every slot keeps its recorded batch and work
+ * queue, so a caller can alternate steps recorded over different buffers
+ * (one step's copies overlapping the other's kernels).  TBG_ERR_STATE while
+ * a batch is being recorded. */
+int tbg_batch_select(int slot);
+
+/* Persistent-launch configuration of every slot: CTAs per SM (default 4),
+ * and the iteration bound of a dependency wait (<= 0 keeps the current
+ * one). */
 int tbg_batch_tune(int ctas_per_sm, long long spin_limit);
 
 /* dst = a & ~b over `bytes` (a multiple of 16) of explicit device buffers:

@@ -74,6 +74,13 @@ def lib():
             "tbg_batch_run": [i],
             "tbg_batch_counts": [C.POINTER(u64), i],
             "tbg_batch_tune": [i, C.c_longlong],
+            "tbg_batch_select": [i],
+            "tbg_batch_count": [i],
+            "tbg_mark": [C.POINTER(u64)],
+            "tbg_copy_in": [vp, vp, sz, u64, C.POINTER(u64)],
+            "tbg_copy_out": [vp, vp, sz, u64, C.POINTER(u64)],
+            "tbg_join": [u64],
+            "tbg_wait_ticket": [u64, i],
             "tbg_table_build": [C.c_char_p, u64, i, i, C.POINTER(vp), C.POINTER(u64)],
             "tbg_table_free_host": [vp],
             "tbg_probe_open": [vp, u64, C.c_char_p, C.POINTER(i)],
@@ -281,6 +288,50 @@ def batch_counts(n: int):
 
 def batch_tune(ctas_per_sm: int, spin_limit: int = 0):
     check(lib().tbg_batch_tune(ctas_per_sm, spin_limit))
+
+
+def batch_select(slot: int):
+    """Batch slot (0..3) that recording and runs act on."""
+    check(lib().tbg_batch_select(slot))
+
+
+# ------------------------------------------------------- copy streams, tickets
+def mark() -> int:
+    """Ticket of the library stream's current point."""
+    t = C.c_uint64()
+    check(lib().tbg_mark(C.byref(t)))
+    return t.value
+
+
+def _nbytes(t) -> int:
+    return t.numel() * t.element_size()
+
+
+def copy_in(dev, host, after: int = 0, ticket: bool = False):
+    """Host-to-device copy (pinned host tensor -> device tensor of the same
+    size) on the inbound copy stream after ticket `after`; returns the
+    ticket after it when asked."""
+    t = C.c_uint64()
+    check(lib().tbg_copy_in(ptr(dev), ptr(host), _nbytes(host), after,
+                            C.byref(t) if ticket else None))
+    return t.value if ticket else None
+
+
+def copy_out(host, dev, after: int = 0, ticket: bool = False):
+    """Device-to-host copy on the outbound copy stream after ticket `after`."""
+    t = C.c_uint64()
+    check(lib().tbg_copy_out(ptr(host), ptr(dev), _nbytes(dev), after,
+                             C.byref(t) if ticket else None))
+    return t.value if ticket else None
+
+
+def join(ticket: int):
+    """Later work on the library stream waits for the ticket."""
+    check(lib().tbg_join(ticket))
+
+
+def wait_ticket(ticket: int, timeout_ms: int = 0):
+    check(lib().tbg_wait_ticket(ticket, timeout_ms))
 
 
 # ---------------------------------------------------------------- table probes

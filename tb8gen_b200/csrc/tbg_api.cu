@@ -545,7 +545,7 @@ static int launch_op(const Op &o) {
 
 static int submit(Op &o) {
   o.ntiles = op_tiles(o);
-  if (g_eng.batch.recording) return g_eng.batch.add(o);
+  if (g_eng.batch().recording) return g_eng.batch().add(o);
   return launch_op(o);
 }
 
@@ -692,9 +692,9 @@ static int epilogue(uint8_t *T, const uint8_t *Win, uint8_t *Wout, uint64_t *cnt
   o.wout = reinterpret_cast<uint4 *>(Wout);
   o.n16 = m.d.bytes / 16;
   o.nbits = m.d.ii.size;
-  if (g_eng.batch.recording) {
+  if (g_eng.batch().recording) {
     if (cnt) return fail(TBG_ERR_STATE, "counts of a recorded epilogue come from tbg_batch_counts");
-    o.cnt_slot = g_eng.batch.ncounts++;
+    o.cnt_slot = g_eng.batch().ncounts++;
     o.cnt = nullptr;
     return submit(o);
   }
@@ -791,14 +791,14 @@ extern "C" int tbg_clear(int s) {
 extern "C" int tbg_batch_count(int s) {
   NEED_MAT();
   if (s < -1 || s >= TBG_NSLICES) return fail(TBG_ERR_ARG, "bad slice");
-  if (!g_eng.batch.recording) return fail(TBG_ERR_STATE, "tbg_batch_count records into a batch");
+  if (!g_eng.batch().recording) return fail(TBG_ERR_STATE, "tbg_batch_count records into a batch");
   Material &m = g_eng.mats[g_eng.cur];
   if (!m.slot[s + 1]) return fail(TBG_ERR_UNBOUND, "slice %d not bound", s);
   Op o = new_op(OP_COUNT);
   o.T = reinterpret_cast<uint4 *>(m.slot[s + 1]);
   o.n16 = m.d.bytes / 16;
   o.nbits = m.d.ii.size;
-  o.cnt_slot = g_eng.batch.ncounts++;
+  o.cnt_slot = g_eng.batch().ncounts++;
   return submit(o);
 }
 
@@ -1004,14 +1004,14 @@ int Batch::finish() {
 
 extern "C" int tbg_batch_begin(void) {
   if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
-  if (g_eng.batch.recording) return fail(TBG_ERR_STATE, "already recording");
-  g_eng.batch.clear();
-  g_eng.batch.recording = true;
+  if (g_eng.batch().recording) return fail(TBG_ERR_STATE, "already recording");
+  g_eng.batch().clear();
+  g_eng.batch().recording = true;
   return TBG_OK;
 }
 
 extern "C" int tbg_batch_end(int *nops, uint64_t *nitems) {
-  Batch &b = g_eng.batch;
+  Batch &b = g_eng.batch();
   if (!b.recording) return fail(TBG_ERR_STATE, "not recording");
   b.recording = false;
   if (b.ops.empty()) return fail(TBG_ERR_ARG, "empty batch");
@@ -1022,15 +1022,25 @@ extern "C" int tbg_batch_end(int *nops, uint64_t *nitems) {
   return TBG_OK;
 }
 
+extern "C" int tbg_batch_select(int slot) {
+  if (slot < 0 || slot >= Engine::kBatchSlots) return fail(TBG_ERR_ARG, "batch slot 0..%d", Engine::kBatchSlots - 1);
+  for (const Batch &b : g_eng.batches)
+    if (b.recording) return fail(TBG_ERR_STATE, "a batch is being recorded");
+  g_eng.bslot = slot;
+  return TBG_OK;
+}
+
 extern "C" int tbg_batch_tune(int ctas_per_sm, long long spin_limit) {
   if (ctas_per_sm < 1 || ctas_per_sm > 32) return fail(TBG_ERR_ARG, "ctas_per_sm 1..32");
-  g_eng.batch.ctas_per_sm = ctas_per_sm;
-  if (spin_limit > 0) g_eng.batch.spin_limit = spin_limit;
+  for (Batch &b : g_eng.batches) {
+    b.ctas_per_sm = ctas_per_sm;
+    if (spin_limit > 0) b.spin_limit = spin_limit;
+  }
   return TBG_OK;
 }
 
 extern "C" int tbg_batch_run(int mode) {
-  Batch &b = g_eng.batch;
+  Batch &b = g_eng.batch();
   if (!b.ready) return fail(TBG_ERR_STATE, "no recorded batch");
   cudaStream_t st = g_eng.stream;
   CK(cudaMemsetAsync(b.d_counts, 0, std::max(b.ncounts, 1) * sizeof(unsigned long long), st));
@@ -1055,7 +1065,7 @@ extern "C" int tbg_batch_run(int mode) {
 }
 
 extern "C" int tbg_batch_counts(uint64_t *out, int n) {
-  Batch &b = g_eng.batch;
+  Batch &b = g_eng.batch();
   if (!b.ready || !out || n < 0 || n > b.ncounts) return fail(TBG_ERR_ARG, "bad count request");
   if (n == 0) return TBG_OK;
   int rc = g_eng.wait(0);
@@ -1065,7 +1075,7 @@ extern "C" int tbg_batch_counts(uint64_t *out, int n) {
 }
 
 extern "C" int tbg_batch_counts_async(uint64_t *host_out, int n) {
-  Batch &b = g_eng.batch;
+  Batch &b = g_eng.batch();
   if (!b.ready || !host_out || n < 0 || n > b.ncounts) return fail(TBG_ERR_ARG, "bad count request");
   if (n == 0) return TBG_OK;
   CK(cudaMemcpyAsync(host_out, b.d_counts, n * sizeof(uint64_t), cudaMemcpyDeviceToHost,

@@ -94,7 +94,11 @@ struct Engine {
   int bps_scatter = 8;    // grid = SMs x this for the sparse kernels (tiles loop)
   int bps_verify = 8;
   int max_split = 64;     // parts per tile for small bitmaps (tbg_tune_split)
-  Batch batch;
+  // Recorded batches: kBatchSlots slots, one selected (tbg_batch_select).
+  static constexpr int kBatchSlots = 4;
+  Batch batches[kBatchSlots];
+  int bslot = 0;
+  Batch &batch() { return batches[bslot]; }
   // Host-tier copy streams (inbound, outbound) and the event ring behind
   // tickets: ticket t is event t % kTickets until kTickets later ones exist.
   static constexpr uint64_t kTickets = 8192;
