@@ -748,11 +748,23 @@ def run_probe(a, rank, world, local):
     ms = max_over_ranks(ms, world)
     value = ps.positions * world / (ms / 1e3)
 
-    # dominant kernel: the block decode (k_probe_decode), one touched block =
-    # 64 KiB read; its device time from the library's events
+    # dominant kernel: the block decode (k_probe_decode): a touched block's
+    # stream is read once, from its start (found at open) to the block's
+    # end; its device time from the library's events
     dec_ms = statistics.median(sum(p[0][1] for p in step) for step in phases)
     touched = sum(p[1] for p in phases[-1])
-    alg = touched * PROBE_BLOCK
+
+    def mean_stream(t):
+        sb = nb = 0
+        for side in (0, 1):
+            try:
+                sb += t.stream_bytes(side)
+                nb += t.layout(side)[1]
+            except tbg.TbgError:
+                break
+        return sb / max(nb, 1)
+
+    alg = int(sum(phases[-1][i][1] * mean_stream(t) for i, (_, t, _, _) in enumerate(ps.items)))
     peak, peak_kind = measured_peak()
     achieved = alg / (dec_ms / 1e3) / 1e9
     tr = committed_traffic("k_probe_decode")
@@ -761,8 +773,9 @@ def run_probe(a, rank, world, local):
                 "peak_source": peak_kind, "alg_bytes_per_launch": alg,
                 "traffic": int(tr * touched) if tr else None,
                 "issue_active_frac": committed_issue("k_probe_decode"),
-                "note": "algorithmic bytes = touched blocks x 64 KiB (each read once); "
-                        "the rANS steps, not HBM, bound this kernel"}
+                "note": "algorithmic bytes = touched blocks x their tables' mean stream "
+                        "bytes per block (each stream read once; the zero padding in front "
+                        "of a stream is skipped); the rANS steps, not HBM, bound this kernel"}
     phase = {m: {"locate_ms": round(statistics.median(s[i][0][0] for s in phases), 3),
                  "decode_ms": round(statistics.median(s[i][0][1] for s in phases), 3),
                  "answer_ms": round(statistics.median(s[i][0][2] for s in phases), 3),

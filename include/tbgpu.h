@@ -368,6 +368,13 @@ int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t n, void *d
 int tbg_probe_layout(int handle, int side, uint64_t *data_offset, uint64_t *nblocks,
                      uint64_t *positions);
 
+/* Bytes of one side's compressed streams: per block, from the stream's
+ * first word (its first nonzero 32-bit word, where decompress_rans starts,
+ * probe.c:1362-1372) to the block's end, summed.  tbg_probe_open finds
+ * every block's start once, so that decodes skip the zero padding in front
+ * of the streams; no counterpart in the reference. */
+int tbg_probe_stream_bytes(int handle, int side, uint64_t *bytes);
+
 /* Device time of the phases of the handle's last grouped batch (CUDA
  * events on the library's stream): ms[0] locate and scan, ms[1] the block
  * decodes, ms[2] the answers; *touched_blocks (may be NULL) the blocks it

@@ -90,6 +90,7 @@ def lib():
             "tbg_capture_material": [i, C.c_char_p, i],
             "tbg_tune_split": [i],
             "tbg_probe_phase_ms": [i, C.POINTER(C.c_float), C.POINTER(u64)],
+            "tbg_probe_stream_bytes": [i, i, C.POINTER(u64)],
             "tbg_probe_layout": [i, i, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)],
             "tbg_probe_wdl_batch": [i, vp, u64, vp, i],
             "tbg_encode_batch": [i, vp, u64, vp, vp],
@@ -389,6 +390,12 @@ class DeviceTable:
         a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
         check(lib().tbg_probe_layout(self.handle, side, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def stream_bytes(self, side: int) -> int:
+        """Bytes of one side's compressed streams (zero padding excluded)."""
+        b = C.c_uint64()
+        check(lib().tbg_probe_stream_bytes(self.handle, side, C.byref(b)))
+        return b.value
 
     def phase_ms(self):
         """((locate, decode, answer) device ms, touched blocks) of the last

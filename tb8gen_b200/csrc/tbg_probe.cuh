@@ -23,6 +23,7 @@ struct ProbeSide {
   const uint8_t *index;     // 6 B per 2^idx_bits positions
   const uint8_t *sizes;     // u16 per block: positions in the block - 1
   const uint8_t *data;      // blocks of 2^block_size bytes
+  const uint16_t *start;    // per block: word offset of its stream (k_block_starts), or null
   const RansEntry *entry;   // decode table (device copy)
   const uint16_t *freq;
   const uint8_t *sympat;    // 3 B per symbol (inside the table)
@@ -148,6 +149,49 @@ __device__ __forceinline__ void dev_dec_init(uint64_t &x, const uint8_t *&p, con
   p += 8;
 }
 
+// dev_dec_init from the block's start offset found at open (k_block_starts):
+// the same first word, without reading the block's zero padding again.
+__device__ __forceinline__ void dev_dec_start(const ProbeSide &S, uint32_t block, uint64_t &x,
+                                              const uint8_t *&p, const uint8_t *end) {
+  if (S.start == nullptr) {
+    dev_dec_init(x, p, end);
+    return;
+  }
+  p += 4 * (uint32_t)S.start[block];
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(p);
+  x = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+  p += 8;
+}
+
+// dev_dec_init's scan for every block of one side, once per opened table:
+// the word where the block's stream begins, i.e. its first nonzero 32-bit
+// word, or the word 8 bytes before the block's end if that comes first
+// (where the scan stops).  One warp per block, 512 bytes per step.
+__global__ void __launch_bounds__(256) k_block_starts(ProbeSide S, uint16_t *start) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t nwords = 1u << (S.block_size - 2);
+  const uint32_t limit = nwords - 2;
+  for (uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; b < S.nblocks;
+       b += nwarps) {
+    const uint4 *c = reinterpret_cast<const uint4 *>(S.data + (b << S.block_size));
+    uint32_t found = limit;
+    for (uint32_t w0 = 0; w0 < limit; w0 += 128) {
+      const uint32_t w = w0 + 4 * lane;
+      const uint4 v = w < nwords ? c[w >> 2] : make_uint4(0, 0, 0, 0);
+      const int first = v.x ? 0 : v.y ? 1 : v.z ? 2 : v.w ? 3 : 4;
+      const unsigned m = __ballot_sync(0xffffffffu, first < 4);
+      if (m) {
+        const int l = __ffs(m) - 1;
+        const int f = __shfl_sync(0xffffffffu, first, l);
+        found = min(w0 + 4u * l + (uint32_t)f, limit);
+        break;
+      }
+    }
+    if (lane == 0) start[b] = (uint16_t)found;
+  }
+}
+
 __device__ __forceinline__ void dev_dec_renorm(uint64_t &x, const uint8_t *&p) {
   if (x < kRansL) {
     x = (x << 32) | *reinterpret_cast<const uint32_t *>(p);
@@ -165,7 +209,7 @@ __device__ __forceinline__ int probe_one(const ProbeSide &S, uint64_t idx) {
   const uint8_t *p = S.data + ((size_t)block << S.block_size);
   const uint8_t *end = p + ((size_t)1 << S.block_size);
   uint64_t x;
-  dev_dec_init(x, p, end);
+  dev_dec_start(S, block, x, p, end);
   int sym = 0;
   for (; lit < 0 && p < end; lit += S.symlen[sym] + 1) {
     sym = rans_dec_get(x, S.entry, S.freq);
@@ -387,7 +431,7 @@ __global__ void __launch_bounds__(256) k_probe_decode(ProbeSide S, const uint32_
     const uint8_t *p = S.data + ((size_t)block << S.block_size);
     const uint8_t *end = p + ((size_t)1 << S.block_size);
     uint64_t x;
-    dev_dec_init(x, p, end);
+    dev_dec_start(S, block, x, p, end);
     // cur: the chunk of the next word (word ci of it); nxt: the chunk after
     const uint32_t *wp = reinterpret_cast<const uint32_t *>(p);
     const uint32_t *wend = reinterpret_cast<const uint32_t *>(end);

@@ -324,6 +324,8 @@ struct ProbeHandle {
   Spec sp;
   const uint8_t *base = nullptr;  // the table image
   void *dev_alloc = nullptr;   // decode tables and symlen of both sides
+  uint16_t *dev_starts = nullptr;  // stream start of every block (k_block_starts)
+  uint64_t stream_bytes[2] = {0, 0};  // per side: bytes from each stream's start to its block's end
   uint64_t nkeys = 0;
   // scratch, grown on demand
   uint32_t *key = nullptr, *lit = nullptr;
@@ -469,6 +471,30 @@ static int open_table(const uint8_t *dev_table, uint64_t bytes, const char *mate
       if (ps[b].dt.freq[s]) S.nsym_emit = s + 1;
   }
   if (sides == 1) H.P.side[1] = ProbeSide();
+  // where every block's stream begins: the decoders' zero-padding scan, done
+  // once here (block offsets in 32-bit words fit 16 bits up to 256 KiB blocks)
+  if (H.P.side[0].block_size >= 4 && H.P.side[0].block_size <= 18 &&
+      (sides == 1 || H.P.side[1].block_size == H.P.side[0].block_size)) {
+    const uint64_t nb = H.P.side[0].nblocks + (sides == 2 ? H.P.side[1].nblocks : 0);
+    PCK(cudaMalloc(&H.dev_starts, std::max<uint64_t>(nb, 1) * sizeof(uint16_t)));
+    uint16_t *st = H.dev_starts;
+    for (int b = 0; b < sides; b++) {
+      ProbeSide &S = H.P.side[b];
+      k_block_starts<<<g_eng.num_sms * 8, 256, 0, g_eng.stream>>>(S, st);
+      int rc = g_eng.check_launch("k_block_starts");
+      if (rc) return rc;
+      S.start = st;
+      st += S.nblocks;
+    }
+    PCK(cudaStreamSynchronize(g_eng.stream));
+    std::vector<uint16_t> hs(nb);
+    PCK(cudaMemcpy(hs.data(), H.dev_starts, nb * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    uint64_t i = 0;
+    for (int b = 0; b < sides; b++) {
+      const uint64_t bytes = 1ull << H.P.side[b].block_size;
+      for (uint64_t k = 0; k < H.P.side[b].nblocks; k++, i++) H.stream_bytes[b] += bytes - 4ull * hs[i];
+    }
+  }
   H.P.num = num;
   H.P.symmetric = !split;
   memcpy(H.P.pt, H.sp.pt, 8);
@@ -651,7 +677,7 @@ extern "C" int tbg_probe_close(int handle) {
   cudaStreamSynchronize(g_eng.stream);
   for (auto &e : H.ev)
     if (e) cudaEventDestroy(e);
-  for (void *p : {(void *)H.dev_alloc, (void *)H.key, (void *)H.lit, (void *)H.count,
+  for (void *p : {(void *)H.dev_alloc, (void *)H.dev_starts, (void *)H.key, (void *)H.lit, (void *)H.count,
                   (void *)H.minlit, (void *)H.tpos, (void *)H.list, (void *)H.tile,
                   (void *)H.bounds, (void *)H.symbuf})
     if (p) cudaFree(p);
@@ -727,6 +753,16 @@ extern "C" int tbg_probe_layout(int handle, int side, uint64_t *data_offset, uin
   if (data_offset) *data_offset = (uint64_t)(S.data - H.base);
   if (nblocks) *nblocks = S.nblocks;
   if (positions) *positions = S.ei.size;
+  return TBG_OK;
+}
+
+extern "C" int tbg_probe_stream_bytes(int handle, int side, uint64_t *bytes) {
+  if (handle < 0 || handle >= 8 || !g_probe[handle].used || side < 0 || side > 1 || !bytes)
+    return fail(TBG_ERR_ARG, "bad handle/side");
+  const ProbeHandle &H = g_probe[handle];
+  if (side == 1 && !H.P.side[1].nblocks) return fail(TBG_ERR_ARG, "the table has one side");
+  if (!H.dev_starts) return fail(TBG_ERR_STATE, "block starts not computed for this table");
+  *bytes = H.stream_bytes[side];
   return TBG_OK;
 }
 

@@ -141,3 +141,23 @@ def test_invalid_queries(env):
             out = torch.zeros(4, dtype=torch.int8, device="cuda")
             t.probe(dq, out, mode)
             assert (out.cpu().numpy() == -128).all()
+
+
+@pytest.mark.parametrize("material,seed,modulus", SMALL[:2] + [("KQRvKR", 9, 3)])
+def test_block_stream_starts(env, material, seed, modulus):
+    """The stream start of every block, found once at open (the decoders'
+    zero-padding scan: the first nonzero 32-bit word, at most 8 bytes before
+    the block's end), against the same scan over the host-built image."""
+    torch, tb = env
+    host = np.frombuffer(tb.table_build_host(material, seed, modulus), dtype=np.uint8)
+    with tb.DeviceTable(material, seed, modulus) as t:
+        for side in (0, 1):
+            try:
+                off, nb, _ = t.layout(side)
+            except tb.TbgError:
+                break
+            words = host[off: off + nb * 65536].view(np.uint32).reshape(nb, 16384)
+            nz = words != 0
+            first = np.where(nz.any(axis=1), nz.argmax(axis=1), 16382)
+            first = np.minimum(first, 16382)
+            assert t.stream_bytes(side) == int((65536 - 4 * first.astype(np.int64)).sum())
