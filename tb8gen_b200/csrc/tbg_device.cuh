@@ -216,6 +216,70 @@ __device__ __forceinline__ bb unrank_sets(const DIdx &X, const uint32_t *bin,
   return occ;
 }
 
+// The next m-subset of the free squares in colex order, which is the order
+// of the rank of a set (the combinatorial number system of unrank_sets): the
+// lowest square that can move up to the next free square without reaching
+// the set's next square moves there, and the squares below it drop to the
+// lowest free squares.  s holds m >= 1 squares of freeb and is not the last
+// subset.
+__device__ __forceinline__ bb next_colex(bb s, bb freeb) {
+  int passed = 0;
+  for (;;) {
+    const int x = __ffsll((long long)s) - 1;
+    const bb rest = s & (s - 1);
+    const bb up = x == 63 ? 0 : freeb & ~((bit(x) << 1) - 1);
+    if (rest == 0 || (up & (rest & (~rest + 1)) - 1) != 0) {
+      bb low = 0, f = freeb;
+      for (int i = 0; i < passed; i++) {
+        const bb lb = f & (~f + 1);
+        low |= lb;
+        f ^= lb;
+      }
+      return rest | (up & (~up + 1)) | low;
+    }
+    s = rest;
+    passed++;
+  }
+}
+
+// The sets of position idx for a caller that visits consecutive indices:
+// a full unrank where a row starts (the last set's combinations under one
+// placement of the others, or the whole index with a single set), else the
+// next combination of the last set.  `left` (0 at the first call) counts
+// the positions left in the current row; `occ` is the previous call's
+// result.
+template <int NS>
+__device__ __forceinline__ bb walk_sets(const DIdx &X, const uint32_t *bin, uint64_t idx, int k0,
+                                       int k1, bb *set, bb occ, uint64_t &left) {
+  constexpr int L = NS - 1;
+  if (left == 0) {
+    occ = unrank_sets<NS>(X, bin, idx, k0, k1, set);
+    uint64_t off = idx;
+    if (L > 0) {
+      const uint64_t F = X.factor[L > 0 ? L - 1 : 0];
+      const uint64_t row = idx < (1ull << 32)
+                               ? fast_div32((uint32_t)idx, X.fdiv[L > 0 ? L - 1 : 0])
+                               : idx / F;
+      off = idx - row * F;
+      left = F - off;
+    } else {
+      left = X.size - off;
+    }
+  } else {
+    bb last = 0;
+#pragma unroll
+    for (int k = 0; k < NS; k++)
+      if (k == L) last = set[k];
+    const bb nl = next_colex(last, ~(occ & ~last));
+#pragma unroll
+    for (int k = 0; k < NS; k++)
+      if (k == L) set[k] = nl;
+    occ = (occ & ~last) | nl;
+  }
+  left--;
+  return occ;
+}
+
 // Whether a piece of colour `color` attacks square `target` (is_attacked_by,
 // movegen.h:180-188), given each set's type/colour, the king squares and
 // the occupancy.

@@ -903,11 +903,12 @@ __global__ void __launch_bounds__(kThreads) k_calc_sub(SliceJob J, uint32_t *c0,
   for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < nwords;
        w += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t o[5] = {0, 0, 0, 0, 0};
+    bb set[NS], occ = 0;
+    uint64_t left = 0;
     for (int b = 0; b < 32; b++) {
       uint64_t idx = w * 32 + b;
       if (idx >= n) break;
-      bb set[NS];
-      bb occ = unrank_sets<NS>(X, bin, idx, J.k0, J.k1, set);
+      occ = walk_sets<NS>(X, bin, idx, J.k0, J.k1, set, occ, left);
       uint32_t m = 1u << b;
       if (attacked_by<NS>(M, set, J.k0, J.k1, occ, opp, stm)) {
         o[3] |= m;
@@ -941,11 +942,12 @@ __global__ void __launch_bounds__(kThreads) k_calc_illegal(SliceJob J, uint32_t 
   for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < nwords;
        w += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t ow = 0, ob = 0;
+    bb set[NS], occ = 0;
+    uint64_t left = 0;
     for (int b = 0; b < 32; b++) {
       uint64_t idx = w * 32 + b;
       if (idx >= n) break;
-      bb set[NS];
-      bb occ = unrank_sets<NS>(M.ii, bin, idx, J.k0, J.k1, set);
+      occ = walk_sets<NS>(M.ii, bin, idx, J.k0, J.k1, set, occ, left);
       if (attacked_by<NS>(M, set, J.k0, J.k1, occ, J.k1, 0)) ow |= 1u << b;
       if (attacked_by<NS>(M, set, J.k0, J.k1, occ, J.k0, 1)) ob |= 1u << b;
     }

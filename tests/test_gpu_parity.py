@@ -78,7 +78,7 @@ def test_predecessors_sub(torch_cuda, material):
                 assert not rep, f"{material} stm={stm} s={s} legality={legality}: {rep}"
 
 
-@pytest.mark.parametrize("material", ["KRRvKR", "KQRvKRR", "KRvKNN"])
+@pytest.mark.parametrize("material", ["KRRvKR", "KQRvKRR", "KRvKNN", "KRvKNNN"])
 @pytest.mark.parametrize("modulus", [3, 5])
 def test_calc_sub(torch_cuda, material, modulus):
     G, O = GpuSide(material), oracle_for(material)
@@ -91,7 +91,9 @@ def test_calc_sub(torch_cuda, material, modulus):
                 assert np.array_equal(a[i], b[i]), f"{material} s={s} stm={stm} class {i}"
 
 
-@pytest.mark.parametrize("material", ["KRRvKR", "KQRvKRR", "KNBvKB"])
+# KRRRvK: one set, so a slice is a single row of the walk over consecutive
+# indices; KRvKNNN: a three-piece last set (carries across its squares).
+@pytest.mark.parametrize("material", ["KRRvKR", "KQRvKRR", "KNBvKB", "KRRRvK", "KRvKNNN"])
 def test_illegal_and_mate(torch_cuda, material):
     G, O = GpuSide(material), oracle_for(material)
     for s in SLICES:
