@@ -3,7 +3,7 @@
  * calc_sub_kslices, calc_illegal_and_mate, calc_L_n, calc_W_n) as a C host
  * over the tbgpu C ABI, with every king slice resident in HBM.
  *
- *   tbgen [-s seed] [-m 3|5] [-b device_MB] [-S] [-g steps] [-P] [-p] [-n max_ply] MATERIAL
+ *   tbgen [-s seed] [-m 3|5] [-b device_MB] [-S [-H]] [-g steps] [-P] [-p] [-n max_ply] MATERIAL
  *
  * Prints the reference's per-ply counts ("broken_w = ...", "l<n>_<c> = ...",
  * "w<n>_<c> = ...") in the reference's order.
@@ -22,7 +22,8 @@
  * window of slices that follows the schedule's slice order, as the
  * reference's manager does: a slice is brought in before the first step
  * that unmoves into it (or reads it) and written out after the last one.
- * The steps run in segments of -g steps (default 32 for slices up to 16 MB,
+ * The "wins" planes stay in HBM (-H: in the host tier as well).  The steps
+ * run in segments of -g steps (default 32 for slices up to 16 MB,
  * else 8), pipelined: a
  * segment's reads from the host tier and the previous segment's writes
  * overlap the kernels of the segment between them.
@@ -386,6 +387,14 @@ static uint8_t *HP[2][NPLANE], *HS[2][5];
  * epilogue, nor written back; a verify step with no candidates is skipped. */
 static uint8_t hempty[2][NPLANE][NS];
 
+/* The "wins" planes of both sides stay in HBM unless -H: every half-ply
+ * reads a whole wins plane (the W step also rewrites its own), so they are
+ * the largest stream of the host tier, and both fit a B200 even for a
+ * 7-piece material (2 x 71 GB for KRRRvKRRR). */
+static int g_host_wins;
+static uint8_t *g_dwins[2];
+#define DWIN(c, s) (g_dwins[c] + (size_t)(s) * g_bytes)
+
 /* device buffers of the set-up steps (calc_sub, illegal and mate) */
 static uint8_t *setup_bm[4], *setup_sub[5], *setup_base;
 
@@ -402,8 +411,12 @@ static void st_calc_subs(void)
 static void st_illegal_and_mate(void)
 {
   uint64_t cnt[4] = { 0, 0, 0, 0 }, c;
-  uint8_t **b = setup_bm;
+  uint8_t *b[4] = { setup_bm[0], setup_bm[1], setup_bm[2], setup_bm[3] };
   for (int s = 0; s < NS; s++) {
+    if (g_dwins[0]) {
+      b[0] = DWIN(WHITE, s);
+      b[1] = DWIN(BLACK, s);
+    }
     ok(tbg_calc_illegal(s, b[0], b[1]), "illegal");
     ok(tbg_calc_mate(s, b[0], b[1], b[2], b[3]), "mate");
     for (int j = 0; j < 4; j++) {
@@ -413,8 +426,10 @@ static void st_illegal_and_mate(void)
       if (j >= 2) hempty[j - 2][P_LP][s] = c == 0;
     }
     ok(tbg_slot_bind(0, NULL, 0), "unbind");
-    d2h(HSL(P_WINS, WHITE, s), b[0], g_bytes);
-    d2h(HSL(P_WINS, BLACK, s), b[1], g_bytes);
+    if (!g_dwins[0]) {
+      d2h(HSL(P_WINS, WHITE, s), b[0], g_bytes);
+      d2h(HSL(P_WINS, BLACK, s), b[1], g_bytes);
+    }
     d2h(HSL(P_LP, WHITE, s), b[2], g_bytes);
     d2h(HSL(P_LP, BLACK, s), b[3], g_bytes);
   }
@@ -560,7 +575,7 @@ static void prep(const Part *P, int h, int64_t q)
         if (where_[t] >= 0) continue;
         const int b = take(q - 3);
         where_[t] = b;
-        cin(win[b].bm, HSL(P_WINS, stm ^ 1, t), g_bytes);
+        if (!g_dwins[stm ^ 1]) cin(win[b].bm, HSL(P_WINS, stm ^ 1, t), g_bytes);
         cin(win[b].sub, HSUB(stm ^ 1, P->cls, t), g_sub);
       }
       cin(st_src[p][j], HSL(P_X, stm, s), g_bytes);
@@ -581,7 +596,8 @@ static void prep(const Part *P, int h, int64_t q)
     if (P->kind == PART_W)
       for (int x = 0; x < ntouch[stm][k]; x++) {
         const int t = touch[stm][k][x];
-        if (last_use[stm][t] == k && hit[t]) cin(st_win[p][i++], HSL(P_WINS, stm, t), g_bytes);
+        if (last_use[stm][t] == k && hit[t] && !g_dwins[stm])
+          cin(st_win[p][i++], HSL(P_WINS, stm, t), g_bytes);
       }
   }
   ok(tbg_copy_in(NULL, NULL, 0, 0, &in_tk[q % TK_RING]), "fence");
@@ -614,7 +630,8 @@ static void compute(const Part *P, int h, int64_t q)
       rec();
       for (int x = 0; x < ntouch[stm][k]; x++) {
         const int t = touch[stm][k][x];
-        ok(tbg_slot_bind(t, win[where_[t]].bm, g_bytes), "bind");
+        ok(tbg_slot_bind(t, g_dwins[stm ^ 1] ? DWIN(stm ^ 1, t) : win[where_[t]].bm, g_bytes),
+           "bind");
         ok(tbg_sub_bind(t, win[where_[t]].sub, g_sub), "bind sub");
       }
       ok(tbg_slot_bind(-1, st_src[p][j], g_bytes), "bind");
@@ -648,9 +665,9 @@ static void compute(const Part *P, int h, int64_t q)
         const int t = touch[stm][k][x];
         if (last_use[stm][t] != k || !hit[t]) continue;
         rec();
-        ok(tbg_epilogue_W_to(t, st_win[p][i], st_win[p][i], NULL), "epilogue");
+        uint8_t *wb = g_dwins[stm] ? DWIN(stm, t) : st_win[p][i++];
+        ok(tbg_epilogue_W_to(t, wb, wb, NULL), "epilogue");
         cnt_slice[ncnt + nc++] = t;
-        i++;
       }
   }
   if (g_recording) {
@@ -679,7 +696,7 @@ static void compute(const Part *P, int h, int64_t q)
       if (P->kind == PART_W) {
         if (hit[t]) {
           cout_(HSL(P_WC, stm, t), win[where_[t]].bm, g_bytes);
-          cout_(HSL(P_WINS, stm, t), st_win[p][i++], g_bytes);
+          if (!g_dwins[stm]) cout_(HSL(P_WINS, stm, t), st_win[p][i++], g_bytes);
         } else {
           hempty[stm][P_WC][t] = 1;
         }
@@ -770,8 +787,11 @@ static void st_setup(void)
   if (g_seg == 0) g_seg = g_bytes <= (16u << 20) ? 32 : 8;
   init_king_tables();
   init_schedule();
+  if (!g_host_wins && tbg_alloc((size_t)2 * NS * g_bytes, (void **)&g_dwins[0]) == TBG_OK)
+    g_dwins[1] = g_dwins[0] + (size_t)NS * g_bytes;
   for (int c = 0; c < 2; c++) {
-    for (int p = 0; p < NPLANE; p++) HP[c][p] = host_alloc((size_t)g_bytes * NS);
+    for (int p = 0; p < NPLANE; p++)
+      if (p != P_WINS || !g_dwins[0]) HP[c][p] = host_alloc((size_t)g_bytes * NS);
     for (int k = 0; k < 5; k++) HS[c][k] = host_alloc((size_t)g_sub * NS);
   }
   hcnt = host_alloc(NS * sizeof *hcnt);
@@ -785,7 +805,8 @@ static void st_setup(void)
   ok(tbg_alloc(4 * g_bytes + 5 * g_sub, (void **)&setup_base), "alloc");
   for (int j = 0; j < 4; j++) setup_bm[j] = setup_base + j * g_bytes;
   for (int k = 0; k < 5; k++) setup_sub[k] = setup_base + 4 * g_bytes + k * g_sub;
-  const size_t per_set = (size_t)g_seg * (g_bytes + 2 * g_sub) + (size_t)g_lw * g_bytes;
+  const int nwin_stage = g_dwins[0] ? 0 : g_lw;
+  const size_t per_set = (size_t)g_seg * (g_bytes + 2 * g_sub) + (size_t)nwin_stage * g_bytes;
   for (int p = 0; p < NPAR; p++) {
     uint8_t *base;
     ok(tbg_alloc(per_set, (void **)&base), "alloc");
@@ -798,7 +819,7 @@ static void st_setup(void)
       base += g_sub;
     }
     st_win[p] = calloc(g_lw, sizeof *st_win[p]);
-    for (int i = 0; i < g_lw; i++) {
+    for (int i = 0; i < nwin_stage; i++) {
       st_win[p][i] = base;
       base += g_bytes;
     }
@@ -806,8 +827,11 @@ static void st_setup(void)
   for (int s = 0; s < NS; s++) where_[s] = -1;
   if (!quiet)
     fprintf(stderr,
-            "tbgen: streamed, segments of %d steps, schedule window %d slices, host tier %.1f GB\n",
-            g_seg, window_max, (double)(NPLANE * g_bytes + 5 * g_sub) * NS * 2 / 1e9);
+            "tbgen: streamed, segments of %d steps, schedule window %d slices, host tier %.1f GB, "
+            "wins planes %s\n",
+            g_seg, window_max,
+            (double)((NPLANE - (g_dwins[0] ? 1 : 0)) * g_bytes + 5 * g_sub) * NS * 2 / 1e9,
+            g_dwins[0] ? "in HBM" : "in the host tier");
 }
 
 /* After the set-up steps (copies on the library stream): the host tier is
@@ -859,20 +883,21 @@ int main(int argc, char **argv)
   uint64_t seed = 1;
   int mod = 3, opt, force_stream = 0, max_ply = 1 << 30;
   double budget_mb = 0;
-  while ((opt = getopt(argc, argv, "s:m:qb:SPpn:g:")) != -1) {
+  while ((opt = getopt(argc, argv, "s:m:qb:SHPpn:g:")) != -1) {
     if (opt == 's') seed = strtoull(optarg, NULL, 10);
     else if (opt == 'm') mod = atoi(optarg);
     else if (opt == 'q') quiet = 1;
     else if (opt == 'b') budget_mb = atof(optarg);
     else if (opt == 'S') force_stream = 1;
     else if (opt == 'P') g_plain = 1;
+    else if (opt == 'H') g_host_wins = 1;
     else if (opt == 'p') g_timing = 1;
     else if (opt == 'n') max_ply = atoi(optarg);
     else if (opt == 'g') g_seg = atoi(optarg);
   }
   if (optind >= argc) {
     fprintf(stderr,
-            "usage: tbgen [-s seed] [-m 3|5] [-b device_MB] [-S] [-g steps] [-P] [-p] [-n max_ply] "
+            "usage: tbgen [-s seed] [-m 3|5] [-b device_MB] [-S [-H]] [-g steps] [-P] [-p] [-n max_ply] "
             "MATERIAL\n");
     return EXIT_FAILURE;
   }

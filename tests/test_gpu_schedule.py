@@ -42,21 +42,23 @@ def test_generation_counts_match_reference(material, path):
     assert got == case["lines"]
 
 
-STREAMED = [("KRvK", 16), ("KRRvK", 16), ("KRvKN", 16), ("KRRvKR", 16), ("KRvKN", 1),
-            ("KRRvKR", 5), ("KQvKR", 64)]
+STREAMED = [("KRvK", 16, False), ("KRRvK", 16, False), ("KRvKN", 16, False),
+            ("KRRvKR", 16, False), ("KRvKN", 1, False), ("KRRvKR", 5, False),
+            ("KQvKR", 64, False), ("KRvKN", 16, True), ("KRRvKR", 5, True), ("KQvKR", 32, True)]
 
 
-@pytest.mark.parametrize("material,seg", STREAMED)
-def test_streamed_generation_counts_match_reference(material, seg):
+@pytest.mark.parametrize("material,seg,host_wins", STREAMED)
+def test_streamed_generation_counts_match_reference(material, seg, host_wins):
     """The same generations with the planes in host memory and a device
     window of slices that follows the schedule (tbgen -S), its steps run in
     pipelined segments of `seg` steps (reads, kernels and writes of adjacent
-    segments overlap on three streams): identical counts."""
+    segments overlap on three streams), the "wins" planes in HBM or, with
+    -H, in the host tier too: identical counts."""
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     case = CASES[material]
-    cmd = [TBGEN, "-S", "-g", str(seg)]
+    cmd = [TBGEN, "-S", "-g", str(seg)] + (["-H"] if host_wins else [])
     if case["seed"] is not None:
         cmd += ["-s", str(case["seed"]), "-m", str(case["mod"])]
     r = subprocess.run(cmd + [material], capture_output=True, text=True, timeout=900)
