@@ -1113,7 +1113,9 @@ def run_fixpoint(a, rank, world, local):
         "data": "synthetic (seeded 7-piece stub; the generation itself is deterministic)",
         "config": {"workload": "fixpoint", "material": mat, "mode": "streamed",
                    "plies": plies, "half_plies": len(times),
-                   "note": "a step is one half-ply (calc_W_n or calc_L_n) over all 462 slices",
+                   "note": "a step is one half-ply (calc_W_n or calc_L_n) over all 462 slices; "
+                           "the W, L, X and capture planes stream through page-locked host "
+                           "memory, the two wins planes stay in HBM",
                    "l2": "slice planes of the whole material stream through the device"},
         "total_s": round(wall, 2), "half_ply_ms_total": round(ms, 1),
         "resident_half_ply_ms_total": round(sum(t for _, t, _ in t2), 1),
@@ -1129,7 +1131,8 @@ def run_fixpoint(a, rank, world, local):
         "e2e": {"value": round(value, 1), "unit": "positions/s",
                 "h2d_bytes_per_step": stats.get("h2d_bytes", 0) // max(len(times), 1),
                 "d2h_bytes_per_step": stats.get("d2h_bytes", 0) // max(len(times), 1),
-                "note": "streamed mode: every slice moves through host memory"},
+                "note": "streamed mode: the W, L, X and capture planes of every slice move "
+                        "through host memory"},
         "cpu_baseline": cpu,
     }
 
