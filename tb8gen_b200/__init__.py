@@ -291,6 +291,11 @@ def batch_tune(ctas_per_sm: int, spin_limit: int = 0):
     check(lib().tbg_batch_tune(ctas_per_sm, spin_limit))
 
 
+def batch_count(s: int):
+    """Records, in the batch being recorded, the count of slot s's bitmap."""
+    check(lib().tbg_batch_count(s))
+
+
 def batch_select(slot: int):
     """Batch slot (0..3) that recording and runs act on."""
     check(lib().tbg_batch_select(slot))

@@ -96,3 +96,78 @@ def test_count_strided(setup):
             bits = np.unpackbits(host[i * stride:i * stride + m.bytes], bitorder="little")
             want += int(bits[:m.size].sum())
         assert tbg.count_strided(dev, stride, n) == want
+
+
+def test_copy_tickets(setup):
+    """Host-tier copies on the library's copy streams, ordered by tickets: a
+    copy in, a kernel joined after it (a count), a copy out after the
+    kernel's mark; a ticket 8192 tickets old is refused."""
+    torch, tbg, jobs, pools, nops = setup
+    m = tbg.Material("KRRvKR").select()
+    rng = np.random.default_rng(11)
+    host = torch.from_numpy(rng.integers(0, 256, size=m.bytes, dtype=np.uint8)).pin_memory()
+    back = torch.zeros(m.bytes, dtype=torch.uint8).pin_memory()
+    dev = torch.zeros(m.bytes, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    first = tbg.mark()
+    t_in = tbg.copy_in(dev, host, first, ticket=True)
+    tbg.join(t_in)
+    tbg.bind(0, dev)
+    got = tbg.count(0)
+    bits = np.unpackbits(host.numpy(), bitorder="little")[:m.size]
+    assert got == int(bits.sum())
+    mk = tbg.mark()
+    t_out = tbg.copy_out(back, dev, mk, ticket=True)
+    tbg.wait_ticket(t_out)
+    assert torch.equal(back, host)
+    for _ in range(8193):
+        tbg.mark()
+    with pytest.raises(tbg.TbgError):
+        tbg.wait_ticket(first)
+    tbg.unbind_all()
+
+
+def test_batch_slots(setup):
+    """Two batches recorded in two slots over different buffers keep their
+    own queues: running slot 1 then slot 0 gives each job's results of its
+    own buffers, equal to slot 0's results when the inputs are equal; a
+    recorded count equals tbg_count of the same bitmap."""
+    torch, tbg, jobs, pools, nops = setup
+    (a, _), ca = run(torch, tbg, jobs, pools, 1)
+    names = ("L_prev", "W_prev", "T", "X")
+    orig = [tuple(getattr(j, n) for n in names) for j in jobs]
+    alt = [(lp.clone(), wp.clone(), torch.zeros_like(t), torch.zeros_like(x))
+           for lp, wp, t, x in orig]
+    from tb8gen_b200.plyjob import record_step
+    try:
+        for j, bufs in zip(jobs, alt):
+            for n, t in zip(names, bufs):
+                setattr(j, n, t)
+        tbg.batch_select(1)
+        record_step(jobs)
+        tbg.batch_run(1)
+        tbg.sync()
+        cb = tbg.batch_counts(len(jobs))
+        tbg.batch_select(0)
+        tbg.batch_run(1)
+        tbg.sync()
+        assert tbg.batch_counts(len(jobs)) == ca == cb
+        for (t0, x0, _), (_, _, t1, x1) in zip(a, alt):
+            assert np.array_equal(t0, t1.cpu().numpy()) and np.array_equal(x0, x1.cpu().numpy())
+        # a recorded count of one job's L bitmap
+        j = jobs[0]
+        j.m.select()
+        tbg.batch_select(2)
+        tbg.batch_begin()
+        tbg.bind(-1, alt[0][3])
+        tbg.batch_count(-1)
+        tbg.batch_end()
+        tbg.batch_run(1)
+        tbg.bind(0, alt[0][3])
+        assert tbg.batch_counts(1)[0] == tbg.count(0)
+    finally:
+        tbg.batch_select(0)
+        for j, bufs in zip(jobs, orig):
+            for n, t in zip(names, bufs):
+                setattr(j, n, t)
+        tbg.unbind_all()
