@@ -221,12 +221,13 @@ __device__ __forceinline__ int probe_one(const ProbeSide &S, uint64_t idx) {
 
 // ------------------------------------------------------------ probe passes
 constexpr uint32_t kNoKey = 0xffffffffu;
+constexpr uint32_t kNoLit = 0xffffffffu;  // minlit of an untouched block
 
 // Pass 1 of a grouped probe (tables whose symbols all cover L positions):
-// block key and symbol-relative position of every query, per-block counts
-// and lowest position.
+// block key and symbol-relative position of every query, and per block the
+// lowest position asked for (which also marks the block touched).
 __global__ void k_probe_locate(ProbeTable P, const Query *q, uint64_t n, uint32_t *key,
-                               uint32_t *lit, uint32_t *count, uint32_t *minlit, int8_t *out) {
+                               uint32_t *lit, uint32_t *minlit, int8_t *out) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     int bside;
@@ -247,16 +248,14 @@ __global__ void k_probe_locate(ProbeTable P, const Query *q, uint64_t n, uint32_
     const uint32_t k = S.key0 + block;
     key[i] = k;
     lit[i] = (uint32_t)l;
-    atomicAdd(&count[k], 1u);
-    atomicMin(&minlit[k], (uint32_t)l);
+    atomicMin(&minlit[k], (uint32_t)l);  // also marks the block touched
   }
 }
 
-// Exclusive scan of the touched flags (count[k] != 0) of the blocks: tpos[k]
+// Exclusive scan of the touched flags (minlit[k] != kNoLit) of the blocks: tpos[k]
 // is block k's place among the touched blocks, list[tpos[k]] = k for the
 // touched ones.  Three passes over tiles of 4096 keys: tile totals, a scan
-// of the totals, then each tile's scan plus its offset.  The query counts
-// ride along (their total is the number of valid queries).
+// of the totals, then each tile's scan plus its offset.
 constexpr int kScanTile = 4096;
 
 struct Pair32 {
@@ -294,16 +293,16 @@ __device__ __forceinline__ Pair32 block_scan(Pair32 v, Pair32 *warp_tot) {
   return v;
 }
 
-__global__ void __launch_bounds__(1024) k_scan_tiles(const uint32_t *count, uint64_t nkeys,
+__global__ void __launch_bounds__(1024) k_scan_tiles(const uint32_t *minlit, uint64_t nkeys,
                                                       uint32_t *tile_cnt, uint32_t *tile_flag) {
   __shared__ Pair32 wt[32];
   const uint64_t base = (uint64_t)blockIdx.x * kScanTile + 4 * threadIdx.x;
   Pair32 v = {0, 0};
   for (int e = 0; e < 4; e++)
     if (base + e < nkeys) {
-      const uint32_t c = count[base + e];
+      const uint32_t c = minlit[base + e] != kNoLit;
       v.a += c;
-      v.b += c != 0;
+      v.b += c;
     }
   v = block_scan(v, wt);
   if (threadIdx.x == 1023) {
@@ -336,7 +335,7 @@ __global__ void __launch_bounds__(1024) k_scan_totals(uint32_t *tile_cnt, uint32
   }
 }
 
-__global__ void __launch_bounds__(1024) k_scan_finish(const uint32_t *count, uint64_t nkeys,
+__global__ void __launch_bounds__(1024) k_scan_finish(const uint32_t *minlit, uint64_t nkeys,
                                                        const uint32_t *tile_flag, uint32_t *tpos,
                                                        uint32_t *list) {
   __shared__ Pair32 wt[32];
@@ -344,7 +343,7 @@ __global__ void __launch_bounds__(1024) k_scan_finish(const uint32_t *count, uin
   uint32_t c[4];
   Pair32 v = {0, 0};
   for (int e = 0; e < 4; e++) {
-    c[e] = base + e < nkeys ? count[base + e] : 0u;
+    c[e] = base + e < nkeys ? (uint32_t)(minlit[base + e] != kNoLit) : 0u;
     v.a += c[e];
     v.b += c[e] != 0;
   }
@@ -473,10 +472,10 @@ __global__ void __launch_bounds__(256) k_probe_decode(ProbeSide S, const uint32_
 // Device-side extent of a batch's touched blocks: bounds[0] = touched
 // blocks, bounds[1] = touched blocks of side 0 (tpos at side 1's first key;
 // key1 == nkeys for a one-sided table).
-__global__ void k_probe_bounds(const uint32_t *count, const uint32_t *tpos, uint64_t nkeys,
+__global__ void k_probe_bounds(const uint32_t *minlit, const uint32_t *tpos, uint64_t nkeys,
                                uint64_t key1, uint32_t *bounds) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const uint32_t total = tpos[nkeys - 1] + (count[nkeys - 1] ? 1u : 0u);
+    const uint32_t total = tpos[nkeys - 1] + (minlit[nkeys - 1] != kNoLit ? 1u : 0u);
     bounds[0] = total;
     bounds[1] = key1 < nkeys ? tpos[key1] : total;
   }

@@ -330,7 +330,7 @@ struct ProbeHandle {
   // scratch, grown on demand
   uint32_t *key = nullptr, *lit = nullptr;
   uint64_t cap_q = 0;
-  uint32_t *count = nullptr, *minlit = nullptr, *tpos = nullptr, *list = nullptr, *tile = nullptr;
+  uint32_t *minlit = nullptr, *tpos = nullptr, *list = nullptr, *tile = nullptr;
   uint8_t *symbuf = nullptr;   // decoded symbols (bytes)
   uint64_t cap_sym = 0;
   // events of the last grouped batch: start, first decode, after the last
@@ -560,7 +560,7 @@ static int decode_async(ProbeHandle &H, uint64_t n, uint32_t W, int8_t *out) {
   int rc = grow_buf(&H.symbuf, &H.cap_sym, (uint64_t)W * per_block);
   if (rc) return rc;
   TS *scratch = reinterpret_cast<TS *>(H.symbuf);
-  k_probe_bounds<<<1, 32, 0, st>>>(H.count, H.tpos, H.nkeys, two ? H.P.side[1].key0 : H.nkeys,
+  k_probe_bounds<<<1, 32, 0, st>>>(H.minlit, H.tpos, H.nkeys, two ? H.P.side[1].key0 : H.nkeys,
                                    H.bounds);
   PCK(cudaEventRecord(H.ev[1], st));
   const uint32_t grid_d = std::min<uint32_t>((W + 255) / 256, g_eng.num_sms * 7);
@@ -594,8 +594,7 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
   if ((rc = grow_buf(&H.lit, &cap, n))) return rc;
   H.cap_q = std::max(H.cap_q, n);
   const uint32_t ntiles = (uint32_t)((H.nkeys + kScanTile - 1) / kScanTile);
-  if (!H.count) {
-    PCK(cudaMalloc(&H.count, H.nkeys * sizeof(uint32_t)));
+  if (!H.minlit) {
     PCK(cudaMalloc(&H.minlit, H.nkeys * sizeof(uint32_t)));
     PCK(cudaMalloc(&H.tpos, H.nkeys * sizeof(uint32_t)));
     PCK(cudaMalloc(&H.list, H.nkeys * sizeof(uint32_t)));
@@ -603,12 +602,11 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
     PCK(cudaMalloc(&H.bounds, 2 * sizeof(uint32_t)));
   }
   PCK(cudaEventRecord(H.ev[0], st));
-  PCK(cudaMemsetAsync(H.count, 0, H.nkeys * 4, st));
   PCK(cudaMemsetAsync(H.minlit, 0xff, H.nkeys * 4, st));
-  k_probe_locate<<<grid, 256, 0, st>>>(H.P, q, n, H.key, H.lit, H.count, H.minlit, out);
-  k_scan_tiles<<<ntiles, 1024, 0, st>>>(H.count, H.nkeys, H.tile, H.tile + ntiles);
+  k_probe_locate<<<grid, 256, 0, st>>>(H.P, q, n, H.key, H.lit, H.minlit, out);
+  k_scan_tiles<<<ntiles, 1024, 0, st>>>(H.minlit, H.nkeys, H.tile, H.tile + ntiles);
   k_scan_totals<<<1, 1024, 0, st>>>(H.tile, H.tile + ntiles, ntiles);
-  k_scan_finish<<<ntiles, 1024, 0, st>>>(H.count, H.nkeys, H.tile + ntiles, H.tpos, H.list);
+  k_scan_finish<<<ntiles, 1024, 0, st>>>(H.minlit, H.nkeys, H.tile + ntiles, H.tpos, H.list);
   rc = g_eng.check_launch("probe grouping");
   if (rc) return rc;
   const bool two = H.P.side[1].nblocks != 0;
@@ -632,10 +630,10 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
   // side 0 (tpos at side 1's first key), read by the host to plan the waves
   uint32_t last[3] = {0, 0, 0};
   PCK(cudaMemcpyAsync(&last[0], H.tpos + H.nkeys - 1, 4, cudaMemcpyDeviceToHost, st));
-  PCK(cudaMemcpyAsync(&last[1], H.count + H.nkeys - 1, 4, cudaMemcpyDeviceToHost, st));
+  PCK(cudaMemcpyAsync(&last[1], H.minlit + H.nkeys - 1, 4, cudaMemcpyDeviceToHost, st));
   if (two) PCK(cudaMemcpyAsync(&last[2], H.tpos + H.P.side[1].key0, 4, cudaMemcpyDeviceToHost, st));
   PCK(cudaStreamSynchronize(st));
-  const uint32_t ntouched = last[0] + (last[1] ? 1 : 0);
+  const uint32_t ntouched = last[0] + (last[1] != kNoLit ? 1 : 0);
   const uint32_t nside0 = two ? last[2] : ntouched;
   H.touched = ntouched;
   H.touched_on_device = false;
@@ -677,7 +675,7 @@ extern "C" int tbg_probe_close(int handle) {
   cudaStreamSynchronize(g_eng.stream);
   for (auto &e : H.ev)
     if (e) cudaEventDestroy(e);
-  for (void *p : {(void *)H.dev_alloc, (void *)H.dev_starts, (void *)H.key, (void *)H.lit, (void *)H.count,
+  for (void *p : {(void *)H.dev_alloc, (void *)H.dev_starts, (void *)H.key, (void *)H.lit,
                   (void *)H.minlit, (void *)H.tpos, (void *)H.list, (void *)H.tile,
                   (void *)H.bounds, (void *)H.symbuf})
     if (p) cudaFree(p);
