@@ -320,7 +320,9 @@ int tbg_epilogue_W_static(void *dev_T, const void *dev_wins_in, void *dev_wins_o
  * piece order (the order of main(), tb8gen.c:1331-1339: white king, black
  * king, then knights, bishops, rooks, queens, each type white before
  * black), and the side to move (0 white, 1 black).  16 bytes, like the
- * reference Position's sq[]/stm fields (movegen.h) that probe_table reads. */
+ * reference Position's sq[]/stm fields (movegen.h) that probe_table reads.
+ * Query arrays passed to the probe and encode calls start on a 16-byte
+ * boundary (TBG_ERR_ARG otherwise): each query is read as one vector. */
 typedef struct {
   uint8_t sq[8];
   uint8_t stm;

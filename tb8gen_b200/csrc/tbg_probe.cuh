@@ -56,26 +56,109 @@ struct Query {
 // reference has no such check: its callers only pass legal positions.
 constexpr int8_t kWdlInvalid = -128;
 
+// Byte i of eight squares packed into a 64-bit register.
+__device__ __forceinline__ int pk_get(uint64_t p, int i) { return (int)(p >> (8 * i)) & 0xff; }
+
+// encode_piece (probe.c:603-694, PIECE_ENC) with the squares packed one per
+// byte of a register (byte i: table piece i) and the square tables in
+// shared memory: the steps of the host function in tbg_table.h, without a
+// square array indexed at run time (which would live in local memory).
+__device__ __forceinline__ uint64_t encode_packed(const EncTables &T, const EncInfoP &ei,
+                                                  uint64_t p) {
+  const int n = ei.num;
+  if (p & 0x04) p ^= 0x0707070707070707ull;
+  if (p & 0x20) p ^= 0x3838383838383838ull;
+  const int lim = ei.kk ? 2 : 3;
+  for (int i = 0; i < n; i++) {
+    const int o = T.offdiag[pk_get(p, i)];
+    if (o) {
+      if (o > 0 && i < lim) {
+        uint64_t q = p;
+        for (int j = 0; j < n; j++) {
+          const int sh = 8 * j;
+          q = (q & ~(0xffull << sh)) | ((uint64_t)T.flipdiag[pk_get(p, j)] << sh);
+        }
+        p = q;
+      }
+      break;
+    }
+  }
+  const int p0 = pk_get(p, 0), p1 = pk_get(p, 1), p2 = pk_get(p, 2);
+  uint64_t idx;
+  int k;
+  uint64_t occ = (1ull << p0) | (1ull << p1);
+  if (ei.kk) {
+    idx = (uint64_t)T.kkidx[T.triangle[p0]][p1];
+    k = 2;
+  } else {
+    const int s1 = p1 > p0;
+    const int s2 = (p2 > p0) + (p2 > p1);
+    if (T.offdiag[p0])
+      idx = (uint64_t)T.triangle[p0] * 63 * 62 + (p1 - s1) * 62 + (p2 - s2);
+    else if (T.offdiag[p1])
+      idx = 6 * 63 * 62 + T.diag[p0] * 28 * 62 + T.lower[p1] * 62 + p2 - s2;
+    else if (T.offdiag[p2])
+      idx = 6 * 63 * 62 + 4 * 28 * 62 + T.diag[p0] * 7 * 28 + (T.diag[p1] - s1) * 28 +
+            T.lower[p2];
+    else
+      idx = 6 * 63 * 62 + 4 * 28 * 62 + 4 * 7 * 28 + T.diag[p0] * 7 * 6 +
+            (T.diag[p1] - s1) * 6 + (T.diag[p2] - s2);
+    occ |= 1ull << p2;
+    k = 3;
+  }
+  idx *= ei.factor[0];
+  while (k < n) {
+    const int t = k + ei.norm[k];
+    uint64_t g = 0;
+    for (int i = k; i < t; i++) g |= 1ull << pk_get(p, i);
+    uint64_t sum = 0;
+    int j = 1;
+    for (uint64_t b = g; b; b &= b - 1, j++) {
+      const int sq = __ffsll((long long)b) - 1;
+      sum += T.binom[j][sq - __popcll(occ & ((1ull << sq) - 1))];
+    }
+    idx += sum * ei.factor[k];
+    occ |= g;
+    k = t;
+  }
+  return idx;
+}
+
+// The square tables of a ProbeTable copied into a block's shared memory.
+__device__ __forceinline__ void load_enc_tables(const EncTables *g, EncTables &s) {
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(g);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(&s);
+  for (int i = threadIdx.x; i < (int)(sizeof(EncTables) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
+// A query loaded as one 16-byte vector: squares packed, side to move.
+__device__ __forceinline__ void load_query(const Query *q, uint64_t i, uint64_t &sqs, int &stm) {
+  const uint4 v = reinterpret_cast<const uint4 *>(q)[i];
+  sqs = (uint64_t)v.x | ((uint64_t)v.y << 32);
+  stm = (int)(v.z & 0xff);
+}
+
 // list_squares (probe.c:1511-1520) then encode_piece: table index and side.
 // Returns false for a query that is not a placement (see kWdlInvalid).
-__device__ __forceinline__ bool query_index(const ProbeTable &P, const Query &q, int &bside,
-                                            uint64_t &idx) {
+__device__ __forceinline__ bool query_index(const ProbeTable &P, const EncTables &T, uint64_t sqs,
+                                            int stm, int &bside, uint64_t &idx) {
   uint64_t occ = 0;
   int wk = 0, bk = 0;
   for (int j = 0; j < P.num; j++) {
-    const int sq = q.sq[j];
+    const int sq = pk_get(sqs, j);
     if (sq >= 64 || ((occ >> sq) & 1)) return false;
     occ |= 1ull << sq;
     if (P.pt[j] == 6) wk = sq;
     if (P.pt[j] == 14) bk = sq;
   }
-  if (q.stm > 1) return false;
+  if (stm > 1) return false;
   int flip;
   if (!P.symmetric) {
     flip = 0;
-    bside = q.stm == 1;
+    bside = stm == 1;
   } else {
-    flip = q.stm != 0;
+    flip = stm != 0;
     bside = 0;
   }
   const ProbeSide &S = P.side[bside];
@@ -83,13 +166,17 @@ __device__ __forceinline__ bool query_index(const ProbeTable &P, const Query &q,
     const int df = (wk & 7) - (bk & 7), dr = (wk >> 3) - (bk >> 3);
     if (df >= -1 && df <= 1 && dr >= -1 && dr <= 1) return false;
   }
-  uint8_t p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int fx = flip ? 0x38 : 0x00;
+  uint64_t p = 0;
   for (int i = 0; i < P.num;) {
-    int t = S.ei.pieces[i] ^ (flip << 3);
+    const int t = S.ei.pieces[i] ^ (flip << 3);
     for (int j = 0; j < P.num; j++)
-      if (P.pt[j] == t) p[i++] = q.sq[j] ^ (flip ? 0x38 : 0x00);
+      if (P.pt[j] == t) {
+        p |= (uint64_t)(pk_get(sqs, j) ^ fx) << (8 * i);
+        i++;
+      }
   }
-  idx = encode_piece(*P.T, S.ei, p);
+  idx = encode_packed(T, S.ei, p);
   return idx < S.ei.size;
 }
 
@@ -228,11 +315,14 @@ constexpr uint32_t kNoLit = 0xffffffffu;  // minlit of an untouched block
 // lowest position asked for (which also marks the block touched).
 __global__ void k_probe_locate(ProbeTable P, const Query *q, uint64_t n, uint32_t *key,
                                uint32_t *lit, uint32_t *minlit, int8_t *out) {
+  __shared__ EncTables T;
+  load_enc_tables(P.T, T);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    int bside;
-    uint64_t idx;
-    if (!query_index(P, q[i], bside, idx)) {
+    int bside, stm;
+    uint64_t idx, sqs;
+    load_query(q, i, sqs, stm);
+    if (!query_index(P, T, sqs, stm, bside, idx)) {
       key[i] = kNoKey;
       out[i] = kWdlInvalid;
       continue;
@@ -504,22 +594,28 @@ __global__ void k_probe_answer(ProbeTable P, const uint32_t *key, const uint32_t
 
 // Reference path: every position decoded on its own (any table layout).
 __global__ void k_probe_direct(ProbeTable P, const Query *q, uint64_t n, int8_t *out) {
+  __shared__ EncTables T;
+  load_enc_tables(P.T, T);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    int bside;
-    uint64_t idx;
-    out[i] = query_index(P, q[i], bside, idx) ? (int8_t)probe_one(P.side[bside], idx)
-                                              : kWdlInvalid;
+    int bside, stm;
+    uint64_t idx, sqs;
+    load_query(q, i, sqs, stm);
+    out[i] = query_index(P, T, sqs, stm, bside, idx) ? (int8_t)probe_one(P.side[bside], idx)
+                                                     : kWdlInvalid;
   }
 }
 
 __global__ void k_encode_batch(ProbeTable P, const Query *q, uint64_t n, uint64_t *idx_out,
                                uint8_t *side_out) {
+  __shared__ EncTables T;
+  load_enc_tables(P.T, T);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    int bside = 0;
-    uint64_t idx;
-    const bool ok = query_index(P, q[i], bside, idx);
+    int bside = 0, stm;
+    uint64_t idx, sqs;
+    load_query(q, i, sqs, stm);
+    const bool ok = query_index(P, T, sqs, stm, bside, idx);
     idx_out[i] = ok ? idx : ~0ull;
     if (side_out) side_out[i] = (uint8_t)bside;
   }

@@ -687,6 +687,8 @@ extern "C" int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t
                                    int mode) {
   if (handle < 0 || handle >= 8 || !g_probe[handle].used) return fail(TBG_ERR_ARG, "bad handle");
   if (!dev_queries || !dev_out) return fail(TBG_ERR_ARG, "null buffers");
+  if (reinterpret_cast<uintptr_t>(dev_queries) & 15)
+    return fail(TBG_ERR_ARG, "queries must be 16-byte aligned");
   if (n == 0) return TBG_OK;
   return probe_batch(g_probe[handle], static_cast<const Query *>(dev_queries), n,
                      static_cast<int8_t *>(dev_out), mode);
@@ -695,6 +697,8 @@ extern "C" int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t
 extern "C" int tbg_encode_batch(int handle, const void *dev_queries, uint64_t n, uint64_t *dev_idx,
                                 uint8_t *dev_side) {
   if (handle < 0 || handle >= 8 || !g_probe[handle].used) return fail(TBG_ERR_ARG, "bad handle");
+  if (!dev_queries || (reinterpret_cast<uintptr_t>(dev_queries) & 15))
+    return fail(TBG_ERR_ARG, "queries must be 16-byte aligned");
   k_encode_batch<<<g_eng.num_sms * 8, 256, 0, g_eng.stream>>>(
       g_probe[handle].P, static_cast<const Query *>(dev_queries), n, dev_idx, dev_side);
   return g_eng.check_launch("k_encode_batch");

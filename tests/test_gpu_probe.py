@@ -161,3 +161,20 @@ def test_block_stream_starts(env, material, seed, modulus):
             first = np.where(nz.any(axis=1), nz.argmax(axis=1), 16382)
             first = np.minimum(first, 16382)
             assert t.stream_bytes(side) == int((65536 - 4 * first.astype(np.int64)).sum())
+
+
+def test_misaligned_queries_refused(env):
+    """Query arrays must start on a 16-byte boundary (each query is read as
+    one vector): a misaligned array is refused before any launch."""
+    torch, tb = env
+    with tb.DeviceTable("KRRvK", 5, 3) as t:
+        q = PR.random_queries("KRRvK", 8, 1)
+        buf = torch.zeros(q.size + 16, dtype=torch.uint8, device="cuda")
+        view = buf[1: 1 + q.size]
+        out = torch.zeros(8, dtype=torch.int8, device="cuda")
+        with pytest.raises(tb.TbgError):
+            t.probe(view, out, 0)
+        idx = torch.zeros(8, dtype=torch.int64, device="cuda")
+        side = torch.zeros(8, dtype=torch.uint8, device="cuda")
+        with pytest.raises(tb.TbgError):
+            t.encode(view, idx, side)
