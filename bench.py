@@ -563,10 +563,17 @@ class ProbeSet:
                 raise RuntimeError(f"{failed} draws found no legal {m} position")
             out = torch.empty(per, dtype=torch.int8, device="cuda")
             self.items.append((m, t, q, out))
+        # the workload's queries: the engine's compact 8-byte form (squares
+        # 0-6, side to move); the 16-byte tbg_query form is timed beside it
+        self.q8 = [tbg.compact_queries(q) for _, _, q, _ in self.items]
         self.positions = per * len(self.materials)
         self.table_bytes = sum(t.bytes for _, t, _, _ in self.items)
 
     def probe(self):
+        for (_, t, _, out), q8 in zip(self.items, self.q8):
+            t.probe8(q8, out, 0)
+
+    def probe16(self):
         for _, t, q, out in self.items:
             t.probe(q, out, 0)
 
@@ -747,6 +754,16 @@ def run_probe(a, rank, world, local):
     clk = clocks.stop()
     ms = max_over_ranks(ms, world)
     value = ps.positions * world / (ms / 1e3)
+    # the same batches in the 16-byte query form
+    q0 = torch.cuda.Event(enable_timing=True)
+    q1 = torch.cuda.Event(enable_timing=True)
+    ps.probe16()
+    q0.record(stream)
+    for _ in range(a.steps):
+        ps.probe16()
+    q1.record(stream)
+    torch.cuda.synchronize()
+    ms16 = q0.elapsed_time(q1) / a.steps
 
     # dominant kernel: the block decode (k_probe_decode): a touched block's
     # stream is read once, from its start (found at open) to the block's
@@ -793,7 +810,10 @@ def run_probe(a, rank, world, local):
 
     e2e = None
     if not a.no_e2e:
-        e2e = run_probe_e2e(a, ps, stream)
+        e2e = run_probe_e2e(a, ps, stream, compact=True)
+        e16 = run_probe_e2e(a, ps, stream, compact=False)
+        e2e["value_query16"] = e16["value"]
+        e2e["h2d_bytes_per_step_query16"] = e16["h2d_bytes_per_step"]
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = probe_cpu_baseline(ps, min(a.cpu_seconds, 20.0))
@@ -804,9 +824,11 @@ def run_probe(a, rank, world, local):
         "data": "synthetic (seeded legal positions, seeded synthetic rANS tables)",
         "config": {"workload": "probe", "materials": list(ps.materials),
                    "positions_per_step": ps.positions, "table_bytes": ps.table_bytes,
-                   "block_bytes": PROBE_BLOCK, "seed": PROBE_SEED,
+                   "block_bytes": PROBE_BLOCK, "seed": PROBE_SEED, "query_bytes": 8,
                    "l2": f"inputs larger than L2 ({ps.table_bytes / 1e9:.1f} GB of tables, "
-                         f"{ps.positions * 16 / 1e9:.1f} GB of positions)"},
+                         f"{ps.positions * 8 / 1e9:.1f} GB of positions)"},
+        "value_query16": round(ps.positions * world / (ms16 / 1e3), 1),
+        "ms_per_step_query16": round(ms16, 4),
         "phases": phase, "table_build_s": round(build_s, 2),
         "index_roundtrip": {"ms": round(rt_ms, 3),
                             "positions_per_s": round(ps.positions / (rt_ms / 1e3), 1),
@@ -818,23 +840,26 @@ def run_probe(a, rank, world, local):
     return line
 
 
-def run_probe_e2e(a, ps, stream):
+def run_probe_e2e(a, ps, stream, compact=True):
     """Probe batches through the C ABI from pinned host memory: per step the
-    H2D copy of every query and the D2H copy of every result.  Steps
-    alternate between two device sets of queries and results, so that step
-    i+1's queries go in and step i's results come out on the library's copy
-    streams while the probes between them run.  The host results of the last
-    step are checked against the device's."""
+    H2D copy of every query (8-byte compact form, or the 16-byte tbg_query
+    form) and the D2H copy of every result.  Steps alternate between two
+    device sets of queries and results, so that step i+1's queries go in and
+    step i's results come out on the library's copy streams while the probes
+    between them run.  The host results of the last step are checked against
+    the device's."""
     import torch
 
     import tb8gen_b200 as tbg
 
-    hq = [torch.empty(q.numel(), dtype=torch.uint8, pin_memory=True) for _, _, q, _ in ps.items]
-    for h, (_, _, q, _) in zip(hq, ps.items):
+    qs = ps.q8 if compact else [q for _, _, q, _ in ps.items]
+    hq = [torch.empty(q.numel(), dtype=torch.uint8, pin_memory=True) for q in qs]
+    for h, q in zip(hq, qs):
         h.copy_(q)
-    sets = [[(q, out) for _, _, q, out in ps.items],
-            [(torch.empty_like(q), torch.empty_like(out)) for _, _, q, out in ps.items]]
-    ho = [[torch.empty(o.numel(), dtype=torch.int8, pin_memory=True) for _, o in sets[0]]
+    outs = [out for _, _, _, out in ps.items]
+    sets = [list(zip(qs, outs)),
+            [(torch.empty_like(q), torch.empty_like(o)) for q, o in zip(qs, outs)]]
+    ho = [[torch.empty(o.numel(), dtype=torch.int8, pin_memory=True) for o in outs]
           for _ in range(2)]
     tables = [t for _, t, _, _ in ps.items]
     torch.cuda.synchronize()
@@ -860,7 +885,10 @@ def run_probe_e2e(a, ps, stream):
             if i >= 2:
                 tbg.join(out_t[i - 2])  # set b's results of step i-2 are out
             for t, (q, out) in zip(tables, sets[b]):
-                t.probe(q, out, 0)
+                if compact:
+                    t.probe8(q, out, 0)
+                else:
+                    t.probe(q, out, 0)
             mk[i] = tbg.mark()
             t = 0
             for k, (r, (_, out)) in enumerate(zip(ho[b], sets[b])):
@@ -884,6 +912,7 @@ def run_probe_e2e(a, ps, stream):
     return {"value": round(ps.positions / (ms / 1e3), 1), "unit": "positions/s",
             "ms_per_step": round(ms, 3), "h2d_bytes_per_step": sum(h.numel() for h in hq),
             "d2h_bytes_per_step": sum(r.numel() for r in ho[0]), "steps": steps,
+            "query_bytes": 8 if compact else 16,
             "pipeline": "two query/result sets; copies on the library's copy streams "
                         "overlap the other set's probes"}
 

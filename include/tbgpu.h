@@ -364,6 +364,12 @@ int tbg_probe_close(int handle);
  * stream, or open one handle per concurrent stream). */
 int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t n, void *dev_out, int mode);
 
+/* tbg_probe_wdl_batch on compact queries of 8 bytes (materials of at most 7
+ * pieces): the squares in bytes 0-6 in the order of tbg_query, the side to
+ * move in byte 7; the array 8-byte aligned.  Half the bytes a host feeds per
+ * position; same results.  No counterpart in the reference. */
+int tbg_probe_wdl_batch8(int handle, const void *dev_queries, uint64_t n, void *dev_out, int mode);
+
 /* Where side `side` of an open table keeps its rANS blocks: byte offset of
  * block 0 in the image (block k at data_offset + k * 65536), the number of
  * blocks and of positions (init_table's walk, probe.c:1304-1331). */

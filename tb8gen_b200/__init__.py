@@ -93,6 +93,7 @@ def lib():
             "tbg_probe_stream_bytes": [i, i, C.POINTER(u64)],
             "tbg_probe_layout": [i, i, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)],
             "tbg_probe_wdl_batch": [i, vp, u64, vp, i],
+            "tbg_probe_wdl_batch8": [i, vp, u64, vp, i],
             "tbg_encode_batch": [i, vp, u64, vp, vp],
             "tbg_decode_batch": [i, i, vp, u64, vp],
             "tbg_gen_positions": [C.c_char_p, u64, u64, vp, C.POINTER(C.c_uint32)],
@@ -425,6 +426,11 @@ class DeviceTable:
         n = queries.numel() // QUERY_BYTES
         check(lib().tbg_probe_wdl_batch(self.handle, ptr(queries), n, ptr(out), mode))
 
+    def probe8(self, queries8, out, mode: int = 0):
+        """Probe on compact 8-byte queries (see compact_queries)."""
+        n = queries8.numel() // 8
+        check(lib().tbg_probe_wdl_batch8(self.handle, ptr(queries8), n, ptr(out), mode))
+
     def encode(self, queries, idx, side=None):
         n = queries.numel() // QUERY_BYTES
         check(lib().tbg_encode_batch(self.handle, ptr(queries), n, ptr(idx), ptr(side)))
@@ -435,6 +441,14 @@ class DeviceTable:
 
 def tune_split(max_split: int):
     check(lib().tbg_tune_split(max_split))
+
+
+def compact_queries(queries):
+    """16-byte queries (uint8 tensor) -> 8-byte compact ones: squares 0-6,
+    side to move in byte 7 (materials of at most 7 pieces)."""
+    q = queries.view(-1, QUERY_BYTES)
+    import torch
+    return torch.cat([q[:, :7], q[:, 8:9]], dim=1).contiguous().view(-1)
 
 
 def probe_tune(scratch_bytes: int):

@@ -132,8 +132,17 @@ __device__ __forceinline__ void load_enc_tables(const EncTables *g, EncTables &s
   __syncthreads();
 }
 
-// A query loaded as one 16-byte vector: squares packed, side to move.
-__device__ __forceinline__ void load_query(const Query *q, uint64_t i, uint64_t &sqs, int &stm) {
+// A query loaded as one vector: squares packed, side to move.  A 16-byte
+// query is tbg_query; an 8-byte one (materials of at most 7 pieces) holds
+// the squares in bytes 0-6 and the side to move in byte 7.
+__device__ __forceinline__ void load_query(const Query *q, uint64_t i, int qbytes, uint64_t &sqs,
+                                           int &stm) {
+  if (qbytes == 8) {
+    const uint2 v = reinterpret_cast<const uint2 *>(q)[i];
+    sqs = (uint64_t)v.x | ((uint64_t)(v.y & 0x00ffffffu) << 32);
+    stm = (int)(v.y >> 24);
+    return;
+  }
   const uint4 v = reinterpret_cast<const uint4 *>(q)[i];
   sqs = (uint64_t)v.x | ((uint64_t)v.y << 32);
   stm = (int)(v.z & 0xff);
@@ -313,15 +322,15 @@ constexpr uint32_t kNoLit = 0xffffffffu;  // minlit of an untouched block
 // Pass 1 of a grouped probe (tables whose symbols all cover L positions):
 // block key and symbol-relative position of every query, and per block the
 // lowest position asked for (which also marks the block touched).
-__global__ void k_probe_locate(ProbeTable P, const Query *q, uint64_t n, uint32_t *key,
-                               uint32_t *lit, uint32_t *minlit, int8_t *out) {
+__global__ void k_probe_locate(ProbeTable P, const Query *q, int qbytes, uint64_t n,
+                               uint32_t *key, uint32_t *lit, uint32_t *minlit, int8_t *out) {
   __shared__ EncTables T;
   load_enc_tables(P.T, T);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     int bside, stm;
     uint64_t idx, sqs;
-    load_query(q, i, sqs, stm);
+    load_query(q, i, qbytes, sqs, stm);
     if (!query_index(P, T, sqs, stm, bside, idx)) {
       key[i] = kNoKey;
       out[i] = kWdlInvalid;
@@ -593,14 +602,15 @@ __global__ void k_probe_answer(ProbeTable P, const uint32_t *key, const uint32_t
 }
 
 // Reference path: every position decoded on its own (any table layout).
-__global__ void k_probe_direct(ProbeTable P, const Query *q, uint64_t n, int8_t *out) {
+__global__ void k_probe_direct(ProbeTable P, const Query *q, int qbytes, uint64_t n,
+                               int8_t *out) {
   __shared__ EncTables T;
   load_enc_tables(P.T, T);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     int bside, stm;
     uint64_t idx, sqs;
-    load_query(q, i, sqs, stm);
+    load_query(q, i, qbytes, sqs, stm);
     out[i] = query_index(P, T, sqs, stm, bside, idx) ? (int8_t)probe_one(P.side[bside], idx)
                                                      : kWdlInvalid;
   }
@@ -614,7 +624,7 @@ __global__ void k_encode_batch(ProbeTable P, const Query *q, uint64_t n, uint64_
        i += (uint64_t)gridDim.x * blockDim.x) {
     int bside = 0, stm;
     uint64_t idx, sqs;
-    load_query(q, i, sqs, stm);
+    load_query(q, i, 16, sqs, stm);
     const bool ok = query_index(P, T, sqs, stm, bside, idx);
     idx_out[i] = ok ? idx : ~0ull;
     if (side_out) side_out[i] = (uint8_t)bside;

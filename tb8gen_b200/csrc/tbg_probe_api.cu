@@ -574,13 +574,14 @@ static int decode_async(ProbeHandle &H, uint64_t n, uint32_t W, int8_t *out) {
   return g_eng.check_launch("probe decode");
 }
 
-static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, int mode) {
+static int probe_batch(ProbeHandle &H, const Query *q, int qbytes, uint64_t n, int8_t *out,
+                       int mode) {
   cudaStream_t st = g_eng.stream;
   const int grid = g_eng.num_sms * 8;
   bool grouped = mode == 0 && H.P.side[0].sym_positions > 0 &&
                  (!H.P.side[1].nblocks || H.P.side[1].sym_positions > 0);
   if (!grouped) {
-    k_probe_direct<<<grid, 256, 0, st>>>(H.P, q, n, out);
+    k_probe_direct<<<grid, 256, 0, st>>>(H.P, q, qbytes, n, out);
     return g_eng.check_launch("k_probe_direct");
   }
   if (n >= (1ull << 32)) return fail(TBG_ERR_RANGE, "batch of 2^32 positions or more");
@@ -603,7 +604,7 @@ static int probe_batch(ProbeHandle &H, const Query *q, uint64_t n, int8_t *out, 
   }
   PCK(cudaEventRecord(H.ev[0], st));
   PCK(cudaMemsetAsync(H.minlit, 0xff, H.nkeys * 4, st));
-  k_probe_locate<<<grid, 256, 0, st>>>(H.P, q, n, H.key, H.lit, H.minlit, out);
+  k_probe_locate<<<grid, 256, 0, st>>>(H.P, q, qbytes, n, H.key, H.lit, H.minlit, out);
   k_scan_tiles<<<ntiles, 1024, 0, st>>>(H.minlit, H.nkeys, H.tile, H.tile + ntiles);
   k_scan_totals<<<1, 1024, 0, st>>>(H.tile, H.tile + ntiles, ntiles);
   k_scan_finish<<<ntiles, 1024, 0, st>>>(H.minlit, H.nkeys, H.tile + ntiles, H.tpos, H.list);
@@ -690,7 +691,19 @@ extern "C" int tbg_probe_wdl_batch(int handle, const void *dev_queries, uint64_t
   if (reinterpret_cast<uintptr_t>(dev_queries) & 15)
     return fail(TBG_ERR_ARG, "queries must be 16-byte aligned");
   if (n == 0) return TBG_OK;
-  return probe_batch(g_probe[handle], static_cast<const Query *>(dev_queries), n,
+  return probe_batch(g_probe[handle], static_cast<const Query *>(dev_queries), 16, n,
+                     static_cast<int8_t *>(dev_out), mode);
+}
+
+extern "C" int tbg_probe_wdl_batch8(int handle, const void *dev_queries, uint64_t n,
+                                    void *dev_out, int mode) {
+  if (handle < 0 || handle >= 8 || !g_probe[handle].used) return fail(TBG_ERR_ARG, "bad handle");
+  if (!dev_queries || !dev_out) return fail(TBG_ERR_ARG, "null buffers");
+  if (reinterpret_cast<uintptr_t>(dev_queries) & 7)
+    return fail(TBG_ERR_ARG, "compact queries must be 8-byte aligned");
+  if (g_probe[handle].P.num > 7) return fail(TBG_ERR_ARG, "compact queries hold at most 7 pieces");
+  if (n == 0) return TBG_OK;
+  return probe_batch(g_probe[handle], static_cast<const Query *>(dev_queries), 8, n,
                      static_cast<int8_t *>(dev_out), mode);
 }
 

@@ -178,3 +178,25 @@ def test_misaligned_queries_refused(env):
         side = torch.zeros(8, dtype=torch.uint8, device="cuda")
         with pytest.raises(tb.TbgError):
             t.encode(view, idx, side)
+
+
+def test_compact_queries(env, tmp_path):
+    """8-byte queries (squares 0-6, side to move in byte 7) give the same
+    values as the 16-byte ones, grouped and direct, invalid ones included."""
+    torch, tb = env
+    material, seed, modulus = "KQRvKR", 9, 3
+    with tb.DeviceTable(material, seed, modulus) as t:
+        n = 1 << 18
+        dq = torch.zeros(n * 16, dtype=torch.uint8, device="cuda")
+        assert tb.gen_positions(material, 5, dq) == 0
+        dq.view(n, 16)[:64, 1] = dq.view(n, 16)[:64, 0]   # a few invalid ones
+        q8 = tb.compact_queries(dq)
+        assert q8.numel() == n * 8
+        for mode in (0, 1):
+            a = torch.zeros(n, dtype=torch.int8, device="cuda")
+            b = torch.ones(n, dtype=torch.int8, device="cuda")
+            t.probe(dq, a, mode)
+            t.probe8(q8, b, mode)
+            torch.cuda.synchronize()
+            assert torch.equal(a, b), f"mode {mode}"
+        assert (a[:64] == -128).all()
