@@ -990,10 +990,11 @@ def run_serve(a, rank, world, local):
         tables[m] = tbg.DeviceTable(m, PROBE_SEED, 3)
         q = torch.empty(pool_n * 16, dtype=torch.uint8, device="cuda")
         tbg.gen_positions(m, 4, q)
-        pools[m] = q.cpu().pin_memory()
+        pools[m] = tbg.compact_queries(q).cpu().pin_memory()  # 8-byte queries
         del q
     ex = GpuExecutor(SERVE_PLY, tables, pools, slots=a.serve_slots,
-                     budget_bytes=int(a.serve_budget_gb * 1e9), probe_max=1_000_000)
+                     budget_bytes=int(a.serve_budget_gb * 1e9), probe_max=1_000_000,
+                     query_bytes=8)
     rates = [float(r) for r in a.serve_rates.split(",")]
     base = make_requests(a.serve_jobs, 1.0, SERVE_PLY, PROBE_MATS, seed=4, pool_n=pool_n)
 
@@ -1003,11 +1004,11 @@ def run_serve(a, rank, world, local):
     # warm-up: every table bitmap the stream touches is built once, probe
     # scratch grows to its largest batch
     for m, t in tables.items():
-        q = torch.empty(1_000_000 * 16, dtype=torch.uint8, device="cuda")
-        q.copy_(pools[m][:1_000_000 * 16])
+        q = torch.empty(1_000_000 * 8, dtype=torch.uint8, device="cuda")
+        q.copy_(pools[m][:1_000_000 * 8])
         o = torch.empty(1_000_000, dtype=torch.int8, device="cuda")
         tbg.set_stream(torch.cuda.current_stream())
-        t.probe(q, o, 0)
+        t.probe8(q, o, 0)
         del q, o
     torch.cuda.synchronize()
     t0 = time.time()
@@ -1034,7 +1035,7 @@ def run_serve(a, rank, world, local):
     ply = [r for r in base if r.kind == "ply"]
     prb = [r for r in base if r.kind == "probe"]
     ply_pos = sum(ex.mpools[r.material].m.size for r in ply)
-    h2d = sum(r.n * 16 for r in prb)
+    h2d = sum(r.n * 8 for r in prb)  # compact 8-byte queries
     d2h = sum(2 * ex.mpools[r.material].m.bytes for r in ply) + sum(r.n for r in prb)
     value = top["continuous"]["positions_per_s"]
     peak, peak_kind = measured_peak()

@@ -190,7 +190,8 @@ class GpuExecutor:
     """Runs requests through the C ABI, one CUDA stream per slot."""
 
     def __init__(self, ply_materials, tables: dict, pools: dict, slots: int,
-                 budget_bytes: int, keep_results: bool = False, probe_max: int = 1_000_000):
+                 budget_bytes: int, keep_results: bool = False, probe_max: int = 1_000_000,
+                 query_bytes: int = 16):
         import torch
 
         import tb8gen_b200 as tbg
@@ -203,7 +204,10 @@ class GpuExecutor:
         self.spill_stream = torch.cuda.Stream()
         self.tables = tables                        # material -> DeviceTable (resident)
         self.table_busy = {m: False for m in tables}
-        self.qpool = pools                          # material -> pinned host queries (n*16)
+        self.qpool = pools                          # material -> pinned host queries
+        if query_bytes not in (8, 16):
+            raise ValueError("queries are 16-byte tbg_query or 8-byte compact ones")
+        self.qb = query_bytes
         self.used = sum(t.bytes for t in tables.values())
         self.mpools = {}
         for m in ply_materials:
@@ -237,7 +241,7 @@ class GpuExecutor:
 
     def _job_bytes(self, req):
         if req.kind == "probe":
-            return req.n * 17
+            return req.n * (self.qb + 1)
         m = self.mpools[req.material].m
         need = 5 * m.bytes
         st = self.states.get((req.material, req.slice))
@@ -389,14 +393,18 @@ class GpuExecutor:
         req = job.req
         t = self.tables[req.material]
         self.table_busy[req.material] = True
-        host = self.qpool[req.material][req.offset * 16:(req.offset + req.n) * 16]
-        q = torch.empty(req.n * 16, dtype=torch.uint8, device="cuda")
+        qb = self.qb
+        host = self.qpool[req.material][req.offset * qb:(req.offset + req.n) * qb]
+        q = torch.empty(req.n * qb, dtype=torch.uint8, device="cuda")
         out = torch.empty(req.n, dtype=torch.int8, device="cuda")
         job.bufs = [q, out]
-        job.nbytes = req.n * 17
+        job.nbytes = req.n * (qb + 1)
         self.used += job.nbytes
         q.copy_(host, non_blocking=True)
-        t.probe(q, out, 0)
+        if qb == 8:
+            t.probe8(q, out, 0)
+        else:
+            t.probe(q, out, 0)
         res = torch.empty(req.n, dtype=torch.int8, pin_memory=True)
         res.copy_(out, non_blocking=True)
         job.out = [res]

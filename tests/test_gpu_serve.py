@@ -91,3 +91,20 @@ def test_probe_results_match_direct_probe(server):
     out = torch.empty(5000, dtype=torch.int8, device="cuda")
     ex.tables["KQRvKR"].probe(q, out, 1)
     np.testing.assert_array_equal(recs[0].result, out.cpu().numpy())
+
+
+def test_compact_probe_requests(server):
+    """An executor fed 8-byte compact queries answers a probe batch like the
+    16-byte per-position probe of the same positions."""
+    torch, tbg, ex = server
+    from tb8gen_b200.serve import GpuExecutor, Request, Scheduler
+
+    pools8 = {m: tbg.compact_queries(p.cuda()).cpu().pin_memory() for m, p in ex.qpool.items()}
+    ex8 = GpuExecutor([], ex.tables, pools8, slots=2, budget_bytes=1 << 40, keep_results=True,
+                      probe_max=PROBE_MAX, query_bytes=8)
+    req = Request(0, 0.0, "probe", "KQRvKR", n=3000, offset=77)
+    recs, _ = Scheduler(ex8, 2).run([req])
+    q = ex.qpool["KQRvKR"][77 * 16:(77 + 3000) * 16].cuda()
+    out = torch.empty(3000, dtype=torch.int8, device="cuda")
+    ex.tables["KQRvKR"].probe(q, out, 1)
+    np.testing.assert_array_equal(recs[0].result, out.cpu().numpy())
