@@ -38,3 +38,39 @@ def test_argument_errors_without_gpu():
     n = C.c_uint64()
     assert L.tbg_launches(C.byref(n)) == 0
     assert b"material" in L.tbg_last_error() or L.tbg_last_error() is not None
+
+
+def _tbgen():
+    path = os.path.join(ROOT, "tb8gen_b200", "tbgen")
+    if not os.path.exists(path):
+        import pytest
+        pytest.skip("tbgen not built")
+    return path
+
+
+def test_tbgen_arguments_without_gpu():
+    """The C host driver refuses bad arguments before it touches CUDA: no
+    material, and a segment size outside 0..64."""
+    import subprocess
+
+    tbgen = _tbgen()
+    r = subprocess.run([tbgen], capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "usage: tbgen" in r.stderr
+    for g in ("65", "-1"):
+        r = subprocess.run([tbgen, "-S", "-g", g, "KRvK"], capture_output=True, text=True,
+                           timeout=60)
+        assert r.returncode != 0 and "-g takes" in r.stderr
+
+
+def test_tbgen_reports_library_errors_without_gpu():
+    """Without a GPU, tbg_init fails and the driver exits with the library's
+    message (no CPU fallback)."""
+    import subprocess
+
+    import torch
+
+    if torch.cuda.is_available():
+        import pytest
+        pytest.skip("a GPU is present")
+    r = subprocess.run([_tbgen(), "KRvK"], capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "tbgen: init:" in r.stderr
