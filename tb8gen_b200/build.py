@@ -47,7 +47,7 @@ def build_host(force: bool = False) -> str:
             os.path.getmtime(HOST_OUT) >= max(os.path.getmtime(HOST_SRC), os.path.getmtime(OUT)):
         return HOST_OUT
     cmd = ["gcc", "-std=c11", "-O2", "-Wall", "-o", HOST_OUT, HOST_SRC, "-L" + HERE, "-ltbgpu",
-           "-Wl,-rpath,$ORIGIN"]
+           "-ldl", "-Wl,-rpath,$ORIGIN"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

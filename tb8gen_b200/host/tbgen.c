@@ -3,7 +3,8 @@
  * calc_sub_kslices, calc_illegal_and_mate, calc_L_n, calc_W_n) as a C host
  * over the tbgpu C ABI, with every king slice resident in HBM.
  *
- *   tbgen [-s seed] [-m 3|5] [-b device_MB] [-S [-H]] [-g steps] [-P] [-p] [-n max_ply] MATERIAL
+ *   tbgen [-s seed] [-m 3|5] [-b device_MB] [-S [-H]] [-g steps] [-P] [-p] [-n max_ply]
+ *         [-o dir] MATERIAL
  *
  * Prints the reference's per-ply counts ("broken_w = ...", "l<n>_<c> = ...",
  * "w<n>_<c> = ...") in the reference's order.
@@ -32,16 +33,23 @@
  * persistent kernel (tbg_batch_run mode 1); -P launches every call on its
  * own instead, in the reference's call order.
  *
+ * -o dir writes the reference's per-ply files under dir (n/W/<c>/<wk><bk>,
+ * n/L/..., 0/L and, at the end, 0/wins; write_data's zstd frames), so that
+ * the output can be compared with the reference program's file by file.
+ *
  * -p prints a timing line per half-ply ("time <kind><n>_<c> ms=...").
  * 7-piece capture values come from the seeded stub (tbg_set_stub); a capture
  * that leaves the two kings alone is a draw, as in the reference.
  */
 #define _POSIX_C_SOURCE 200809L
+#include <dlfcn.h>
+#include <errno.h>
 #include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
 #include <time.h>
 #include <unistd.h>
 
@@ -64,6 +72,12 @@ static uint8_t *wins[2][NS], *Wp[2][NS], *Lp[2][NS], *Wc[2][NS], *Lc[2][NS];
 /* capture classes per side (the side to move after the capture) */
 static uint8_t *sub[2][5][NS], *subtmp[NS];
 static int quiet;
+
+/* The reference's per-ply files (-o DIR): defined with the king tables. */
+static const char *g_outdir;
+static void out_plane_dev(int n, const char *name, int stm, uint8_t *const pl[]);
+static void out_plane_host(int n, const char *name, int stm, const uint8_t *plane,
+                           const uint8_t *empty);
 
 static void bind_all(uint8_t *bm[NS], uint8_t *sb[NS])
 {
@@ -118,6 +132,8 @@ static void illegal_and_mate(void)
   printf("broken_w = %llu\nbroken_b = %llu\nl0_w = %llu\nl0_b = %llu\n",
          (unsigned long long)bw, (unsigned long long)bb, (unsigned long long)lw,
          (unsigned long long)lb);
+  if (g_outdir)
+    for (int c = 0; c < 2; c++) out_plane_dev(0, "L", c, Lp[c]);
 }
 
 /* Half-plies of the resident mode run as one recorded batch (a persistent
@@ -194,6 +210,7 @@ static int calc_L_n(int stm, int n, int more_l)
   batch_run();
   cnt = plane_total(Lc[stm]);
   printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
+  if (g_outdir) out_plane_dev(n, "L", stm, Lc[stm]);
   return cnt != 0;
 }
 
@@ -222,6 +239,7 @@ static int calc_W_n(int stm, int n, int more_w)
   }
   for (int s = 0; s < NS; s++) cnt += c[s];
   printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
+  if (g_outdir) out_plane_dev(n, "W", stm, Wc[stm]);
   return cnt != 0;
 }
 
@@ -308,6 +326,104 @@ static void init_king_tables(void)
       }
       KKMap[i][j] = (i == j || (katt(i) >> j & 1)) ? -1 : KKIdx[triangle[s1]][s2];
     }
+}
+
+/* ---- the reference's per-ply files (-o DIR) ----
+ * write_data (util.c:272-343) into the paths of create_name
+ * (kslice.c:306-315): DIR/<n>/<name>/<w|b>/<wk><bk>, each file the slice's
+ * bitmap in chunks of 50 KiB, every chunk one frame: {compressed size, chunk
+ * size, offset} as three size_t, then the chunk compressed by zstd at level
+ * 6, as the reference's Makefile sets it.  libzstd is opened on first use. */
+enum { OUT_CHUNK = 50 * 1024, OUT_LEVEL = 6 };
+static size_t (*z_bound)(size_t);
+static size_t (*z_compress)(void *, size_t, const void *, size_t, int);
+static unsigned (*z_iserror)(size_t);
+static uint8_t *out_frame, *out_host, *out_zero;
+
+static void out_init(void)
+{
+  if (z_compress) return;
+  void *h = dlopen("libzstd.so.1", RTLD_NOW);
+  if (!h) {
+    fprintf(stderr, "tbgen: -o needs libzstd.so.1: %s\n", dlerror());
+    exit(EXIT_FAILURE);
+  }
+  *(void **)&z_bound = dlsym(h, "ZSTD_compressBound");
+  *(void **)&z_compress = dlsym(h, "ZSTD_compress");
+  *(void **)&z_iserror = dlsym(h, "ZSTD_isError");
+  if (!z_bound || !z_compress || !z_iserror) {
+    fprintf(stderr, "tbgen: libzstd.so.1 lacks the compression entry points\n");
+    exit(EXIT_FAILURE);
+  }
+  out_frame = malloc(3 * sizeof(size_t) + z_bound(OUT_CHUNK));
+  out_host = malloc(g_bytes);
+  out_zero = calloc(1, g_bytes);
+  if (!out_frame || !out_host || !out_zero) {
+    fprintf(stderr, "tbgen: out of host memory\n");
+    exit(EXIT_FAILURE);
+  }
+}
+
+static void out_mkdirs(char *path)
+{
+  for (char *p = path + 1; *p; p++)
+    if (*p == '/') {
+      *p = 0;
+      if (mkdir(path, 0777) != 0 && errno != EEXIST) {
+        fprintf(stderr, "tbgen: cannot create %s\n", path);
+        exit(EXIT_FAILURE);
+      }
+      *p = '/';
+    }
+}
+
+static void out_slice(int n, const char *name, int stm, int s, const uint8_t *p)
+{
+  char path[512];
+  const int wk = KKSq[s][0], bk = KKSq[s][1];
+  snprintf(path, sizeof path, "%s/%d/%s/%c/%c%c%c%c", g_outdir, n, name, "wb"[stm],
+           'a' + (wk & 7), '1' + (wk >> 3), 'a' + (bk & 7), '1' + (bk >> 3));
+  out_mkdirs(path);
+  FILE *F = fopen(path, "wb");
+  if (!F) {
+    fprintf(stderr, "tbgen: cannot write %s\n", path);
+    exit(EXIT_FAILURE);
+  }
+  const size_t head = 3 * sizeof(size_t), cap = z_bound(OUT_CHUNK);
+  for (size_t idx = 0; idx < g_bytes; idx += OUT_CHUNK) {
+    const size_t chunk = g_bytes - idx < OUT_CHUNK ? g_bytes - idx : OUT_CHUNK;
+    const size_t c = z_compress(out_frame + head, cap, p + idx, chunk, OUT_LEVEL);
+    if (z_iserror(c)) {
+      fprintf(stderr, "tbgen: zstd failed on %s\n", path);
+      exit(EXIT_FAILURE);
+    }
+    const size_t h3[3] = { c, chunk, idx };
+    memcpy(out_frame, h3, head);
+    if (fwrite(out_frame, 1, head + c, F) != head + c) {
+      fprintf(stderr, "tbgen: cannot write %s\n", path);
+      exit(EXIT_FAILURE);
+    }
+  }
+  fclose(F);
+}
+
+/* A plane whose slices are device buffers (pl[s]). */
+static void out_plane_dev(int n, const char *name, int stm, uint8_t *const pl[])
+{
+  out_init();
+  for (int s = 0; s < NS; s++) {
+    ok(tbg_copy_to_host(out_host, pl[s], g_bytes), "copy to host");
+    out_slice(n, name, stm, s, out_host);
+  }
+}
+
+/* A plane of the host tier; slices flagged empty are zero. */
+static void out_plane_host(int n, const char *name, int stm, const uint8_t *plane,
+                           const uint8_t *empty)
+{
+  out_init();
+  for (int s = 0; s < NS; s++)
+    out_slice(n, name, stm, s, empty && empty[s] ? out_zero : plane + (size_t)s * g_bytes);
 }
 
 /* The slices a step on slice s of side stm touches: s and the slices its
@@ -752,6 +868,7 @@ static int st_calc_W_n(int stm, int n, int more_w)
   Part P = { PART_W, stm, n, more_w, 0, 0 };
   uint64_t cnt = half_ply_count(run_part(&P), stm, P_WC);
   printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
+  if (g_outdir) out_plane_host(n, "W", stm, HP[stm][P_WC], hempty[stm][P_WC]);
   return cnt != 0;
 }
 
@@ -764,6 +881,7 @@ static int st_calc_L_n(int stm, int n, int more_l)
   Part V = { PART_VERIFY, stm, n, more_l, n <= DRAW_RULE ? C_WIN : C_CWIN, done };
   uint64_t cnt = half_ply_count(run_part(&V), stm, P_LC);
   printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
+  if (g_outdir) out_plane_host(n, "L", stm, HP[stm][P_LC], hempty[stm][P_LC]);
   return cnt != 0;
 }
 
@@ -785,7 +903,6 @@ static void *host_alloc(size_t n)
 static void st_setup(void)
 {
   if (g_seg == 0) g_seg = g_bytes <= (16u << 20) ? 32 : 8;
-  init_king_tables();
   init_schedule();
   if (!g_host_wins && tbg_alloc((size_t)2 * NS * g_bytes, (void **)&g_dwins[0]) == TBG_OK)
     g_dwins[1] = g_dwins[0] + (size_t)NS * g_bytes;
@@ -883,7 +1000,7 @@ int main(int argc, char **argv)
   uint64_t seed = 1;
   int mod = 3, opt, force_stream = 0, max_ply = 1 << 30;
   double budget_mb = 0;
-  while ((opt = getopt(argc, argv, "s:m:qb:SHPpn:g:")) != -1) {
+  while ((opt = getopt(argc, argv, "s:m:qb:SHPpn:g:o:")) != -1) {
     if (opt == 's') seed = strtoull(optarg, NULL, 10);
     else if (opt == 'm') mod = atoi(optarg);
     else if (opt == 'q') quiet = 1;
@@ -894,10 +1011,12 @@ int main(int argc, char **argv)
     else if (opt == 'p') g_timing = 1;
     else if (opt == 'n') max_ply = atoi(optarg);
     else if (opt == 'g') g_seg = atoi(optarg);
+    else if (opt == 'o') g_outdir = optarg;
   }
   if (optind >= argc) {
     fprintf(stderr,
             "usage: tbgen [-s seed] [-m 3|5] [-b device_MB] [-S [-H]] [-g steps] [-P] [-p] [-n max_ply] "
+            "[-o dir] "
             "MATERIAL\n");
     return EXIT_FAILURE;
   }
@@ -910,6 +1029,7 @@ int main(int argc, char **argv)
   ok(tbg_set_stub(seed, mod), "stub");
   uint64_t offs[6], capt[6];
   ok(tbg_geometry(&g_size, &g_bytes, &g_sub, offs, capt), "geometry");
+  init_king_tables();
 
   /* resident: 10 bitmap planes, 10 sub planes + temp */
   size_t per = (size_t)g_bytes, persub = (size_t)g_sub;
@@ -922,6 +1042,8 @@ int main(int argc, char **argv)
     st_calc_subs();
     st_illegal_and_mate();
     st_setup_done();
+    if (g_outdir)
+      for (int c = 0; c < 2; c++) out_plane_host(0, "L", c, HP[c][P_LP], hempty[c][P_LP]);
     W = st_calc_W_n;
     L = st_calc_L_n;
   } else {
@@ -978,6 +1100,18 @@ int main(int argc, char **argv)
     }
   }
   ok(tbg_sync(0), "sync");
+  if (g_outdir)
+    for (int c = 0; c < 2; c++) {
+      if (!streamed) {
+        out_plane_dev(0, "wins", c, wins[c]);
+      } else if (g_dwins[c]) {
+        uint8_t *pl[NS];
+        for (int s = 0; s < NS; s++) pl[s] = DWIN(c, s);
+        out_plane_dev(0, "wins", c, pl);
+      } else {
+        out_plane_host(0, "wins", c, HP[c][P_WINS], NULL);
+      }
+    }
   if (g_timing) {
     uint64_t launches = 0;
     ok(tbg_launches(&launches), "launches");
