@@ -1104,7 +1104,9 @@ def run_fixpoint(a, rank, world, local):
         return None
     tbgen = build.build_host()
     mat = a.fix_material
-    base = [tbgen, "-s", "1", "-m", "3", "-p"]
+    # -c 16: a digest of 16 seeded slices of every half-ply's output, so
+    # that the streamed and the resident run are compared slice-exactly
+    base = [tbgen, "-s", "1", "-m", "3", "-p", "-c", "16"]
     if a.fix_max_ply:
         base += ["-n", str(a.fix_max_ply)]
     clocks = ClockSampler(local)
@@ -1151,6 +1153,8 @@ def run_fixpoint(a, rank, world, local):
         "resident_half_ply_ms_total": round(sum(t for _, t, _ in t2), 1),
         "counts_match_resident": counts == counts2 and r2.returncode == 0,
         "count_lines": len(counts), "last_counts": counts[-4:],
+        "slice_digests_compared": sum(1 for c in counts if c.startswith("sum ")),
+        "slices_per_digest": 16,
         "roofline": {"bound": "hbm", "kernel": "half-ply (all kernels)",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 5), "peak_source": peak_kind,

@@ -4,7 +4,7 @@
  * over the tbgpu C ABI, with every king slice resident in HBM.
  *
  *   tbgen [-s seed] [-m 3|5] [-b device_MB] [-S [-H]] [-g steps] [-P] [-p] [-n max_ply]
- *         [-o dir] MATERIAL
+ *         [-o dir] [-c slices] MATERIAL
  *
  * Prints the reference's per-ply counts ("broken_w = ...", "l<n>_<c> = ...",
  * "w<n>_<c> = ...") in the reference's order.
@@ -36,6 +36,9 @@
  * -o dir writes the reference's per-ply files under dir (n/W/<c>/<wk><bk>,
  * n/L/..., 0/L and, at the end, 0/wins; write_data's zstd frames), so that
  * the output can be compared with the reference program's file by file.
+ *
+ * -c K prints after each half-ply a digest of K seeded slices of its output
+ * ("sum <w|l><n>_<c> = <hex>"), to compare runs slice-exactly.
  *
  * -p prints a timing line per half-ply ("time <kind><n>_<c> ms=...").
  * 7-piece capture values come from the seeded stub (tbg_set_stub); a capture
@@ -78,6 +81,50 @@ static const char *g_outdir;
 static void out_plane_dev(int n, const char *name, int stm, uint8_t *const pl[]);
 static void out_plane_host(int n, const char *name, int stm, const uint8_t *plane,
                            const uint8_t *empty);
+
+/* -c K: a digest of K seeded slices of every half-ply's output (defined
+ * with the king tables). */
+static int g_nsum;
+static uint64_t g_sum_seed = 1;
+static void sum_plane_dev(const char *kind, int n, int stm, uint8_t *const pl[]);
+static void sum_plane_host(const char *kind, int n, int stm, const uint8_t *plane,
+                           const uint8_t *empty);
+
+/* A half-ply's output for -o and -c, written after its timing line: the
+ * slices as device buffers (dev) or as a host-tier plane with its empty
+ * flags. */
+static struct {
+  int pending, n, stm;
+  const char *kind, *name;
+  uint8_t *const *dev;
+  const uint8_t *host, *empty;
+} g_last;
+
+static void note_output(const char *kind, const char *name, int n, int stm, uint8_t *const *dev,
+                        const uint8_t *host, const uint8_t *empty)
+{
+  g_last.pending = g_outdir || g_nsum;
+  g_last.kind = kind;
+  g_last.name = name;
+  g_last.n = n;
+  g_last.stm = stm;
+  g_last.dev = dev;
+  g_last.host = host;
+  g_last.empty = empty;
+}
+
+static void emit_output(void)
+{
+  if (!g_last.pending) return;
+  g_last.pending = 0;
+  if (g_last.dev) {
+    if (g_outdir) out_plane_dev(g_last.n, g_last.name, g_last.stm, g_last.dev);
+    if (g_nsum) sum_plane_dev(g_last.kind, g_last.n, g_last.stm, g_last.dev);
+  } else {
+    if (g_outdir) out_plane_host(g_last.n, g_last.name, g_last.stm, g_last.host, g_last.empty);
+    if (g_nsum) sum_plane_host(g_last.kind, g_last.n, g_last.stm, g_last.host, g_last.empty);
+  }
+}
 
 static void bind_all(uint8_t *bm[NS], uint8_t *sb[NS])
 {
@@ -210,7 +257,7 @@ static int calc_L_n(int stm, int n, int more_l)
   batch_run();
   cnt = plane_total(Lc[stm]);
   printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
-  if (g_outdir) out_plane_dev(n, "L", stm, Lc[stm]);
+  note_output("l", "L", n, stm, Lc[stm], NULL, NULL);
   return cnt != 0;
 }
 
@@ -239,7 +286,7 @@ static int calc_W_n(int stm, int n, int more_w)
   }
   for (int s = 0; s < NS; s++) cnt += c[s];
   printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
-  if (g_outdir) out_plane_dev(n, "W", stm, Wc[stm]);
+  note_output("w", "W", n, stm, Wc[stm], NULL, NULL);
   return cnt != 0;
 }
 
@@ -424,6 +471,67 @@ static void out_plane_host(int n, const char *name, int stm, const uint8_t *plan
   out_init();
   for (int s = 0; s < NS; s++)
     out_slice(n, name, stm, s, empty && empty[s] ? out_zero : plane + (size_t)s * g_bytes);
+}
+
+/* ---- digests of seeded slices (-c K) ----
+ * After each half-ply: "sum <w|l><n>_<c> = <hex>", a 64-bit FNV-1a digest
+ * (over 64-bit little-endian words) of the output bitmaps of K slices drawn with splitmix64 from the seed, so
+ * that two runs (resident and streamed) can be compared slice-exactly at
+ * every ply without writing the planes out. */
+static uint64_t sum_mix(uint64_t z)
+{
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+static int sum_slice(int i) { return (int)(sum_mix(g_sum_seed * 1000003u + (uint64_t)i) % NS); }
+
+static uint64_t sum_bytes(uint64_t h, const uint8_t *p, size_t n)
+{
+  for (size_t i = 0; i + 8 <= n; i += 8) {  /* n is a multiple of 64 */
+    uint64_t w;
+    memcpy(&w, p + i, 8);
+    h = (h ^ w) * 0x100000001b3ull;
+  }
+  return h;
+}
+
+static void sum_print(const char *kind, int n, int stm, uint64_t h)
+{
+  printf("sum %s%d_%c = %016llx\n", kind, n, "wb"[stm], (unsigned long long)h);
+}
+
+static void sum_plane_dev(const char *kind, int n, int stm, uint8_t *const pl[])
+{
+  static uint8_t *buf;
+  if (!buf && !(buf = malloc(g_bytes))) {
+    fprintf(stderr, "tbgen: out of host memory\n");
+    exit(EXIT_FAILURE);
+  }
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (int i = 0; i < g_nsum; i++) {
+    ok(tbg_copy_to_host(buf, pl[sum_slice(i)], g_bytes), "copy to host");
+    h = sum_bytes(h, buf, g_bytes);
+  }
+  sum_print(kind, n, stm, h);
+}
+
+static void sum_plane_host(const char *kind, int n, int stm, const uint8_t *plane,
+                           const uint8_t *empty)
+{
+  static uint8_t *zero;
+  if (!zero && !(zero = calloc(1, g_bytes))) {
+    fprintf(stderr, "tbgen: out of host memory\n");
+    exit(EXIT_FAILURE);
+  }
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (int i = 0; i < g_nsum; i++) {
+    const int s = sum_slice(i);
+    h = sum_bytes(h, empty && empty[s] ? zero : plane + (size_t)s * g_bytes, g_bytes);
+  }
+  sum_print(kind, n, stm, h);
 }
 
 /* The slices a step on slice s of side stm touches: s and the slices its
@@ -868,7 +976,7 @@ static int st_calc_W_n(int stm, int n, int more_w)
   Part P = { PART_W, stm, n, more_w, 0, 0 };
   uint64_t cnt = half_ply_count(run_part(&P), stm, P_WC);
   printf("w%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
-  if (g_outdir) out_plane_host(n, "W", stm, HP[stm][P_WC], hempty[stm][P_WC]);
+  note_output("w", "W", n, stm, NULL, HP[stm][P_WC], hempty[stm][P_WC]);
   return cnt != 0;
 }
 
@@ -881,7 +989,7 @@ static int st_calc_L_n(int stm, int n, int more_l)
   Part V = { PART_VERIFY, stm, n, more_l, n <= DRAW_RULE ? C_WIN : C_CWIN, done };
   uint64_t cnt = half_ply_count(run_part(&V), stm, P_LC);
   printf("l%d_%c = %llu\n", n, "wb"[stm], (unsigned long long)cnt);
-  if (g_outdir) out_plane_host(n, "L", stm, HP[stm][P_LC], hempty[stm][P_LC]);
+  note_output("l", "L", n, stm, NULL, HP[stm][P_LC], hempty[stm][P_LC]);
   return cnt != 0;
 }
 
@@ -992,6 +1100,7 @@ static int timed(step_fn f, const char *kind, int stm, int n, int more)
     fprintf(stderr, "time %s%d_%c ms=%.3f positions=%llu\n", kind, n, "wb"[stm], ms,
             (unsigned long long)(g_size * NS));
   }
+  emit_output();  /* -o files and -c digests, outside the timed half-ply */
   return r;
 }
 
@@ -1000,7 +1109,7 @@ int main(int argc, char **argv)
   uint64_t seed = 1;
   int mod = 3, opt, force_stream = 0, max_ply = 1 << 30;
   double budget_mb = 0;
-  while ((opt = getopt(argc, argv, "s:m:qb:SHPpn:g:o:")) != -1) {
+  while ((opt = getopt(argc, argv, "s:m:qb:SHPpn:g:o:c:")) != -1) {
     if (opt == 's') seed = strtoull(optarg, NULL, 10);
     else if (opt == 'm') mod = atoi(optarg);
     else if (opt == 'q') quiet = 1;
@@ -1012,11 +1121,12 @@ int main(int argc, char **argv)
     else if (opt == 'n') max_ply = atoi(optarg);
     else if (opt == 'g') g_seg = atoi(optarg);
     else if (opt == 'o') g_outdir = optarg;
+    else if (opt == 'c') g_nsum = atoi(optarg);
   }
   if (optind >= argc) {
     fprintf(stderr,
             "usage: tbgen [-s seed] [-m 3|5] [-b device_MB] [-S [-H]] [-g steps] [-P] [-p] [-n max_ply] "
-            "[-o dir] "
+            "[-o dir] [-c slices] "
             "MATERIAL\n");
     return EXIT_FAILURE;
   }
@@ -1024,6 +1134,11 @@ int main(int argc, char **argv)
     fprintf(stderr, "tbgen: -g takes 1..%d steps per segment (0: automatic)\n", MAX_SEG);
     return EXIT_FAILURE;
   }
+  if (g_nsum < 0 || g_nsum > NS) {
+    fprintf(stderr, "tbgen: -c takes 0..%d slices\n", NS);
+    return EXIT_FAILURE;
+  }
+  g_sum_seed = seed;
   ok(tbg_init(), "init");
   ok(tbg_material_from_name(argv[optind]), "material");
   ok(tbg_set_stub(seed, mod), "stub");

@@ -66,3 +66,27 @@ def test_streamed_generation_counts_match_reference(material, seg, host_wins):
     assert "streamed" in r.stderr
     got = [l.strip() for l in r.stdout.splitlines() if " = " in l]
     assert got == case["lines"]
+
+
+@pytest.mark.parametrize("material", ["KRRvKR", "KQvKR"])
+def test_streamed_slices_equal_resident(material):
+    """Digests of 16 seeded slices of every half-ply's output (tbgen -c 16)
+    are the same in resident mode, in the streamed pipeline and with the
+    wins planes in the host tier: the modes agree slice by slice, not only
+    in their counts."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    case = CASES[material]
+    base = [TBGEN, "-c", "16"]
+    if case["seed"] is not None:
+        base += ["-s", str(case["seed"]), "-m", str(case["mod"])]
+    outs = []
+    for extra in ([], ["-S", "-g", "5"], ["-S", "-H"]):
+        r = subprocess.run(base + extra + [material], capture_output=True, text=True, timeout=900)
+        assert r.returncode == 0, r.stderr
+        outs.append([l.strip() for l in r.stdout.splitlines() if " = " in l])
+    sums = [l for l in outs[0] if l.startswith("sum ")]
+    # one digest per half-ply: the count lines less the four of the set-up
+    assert sums and len(sums) == len(outs[0]) - len(sums) - 4
+    assert outs[1] == outs[0] and outs[2] == outs[0]
