@@ -183,6 +183,37 @@ def committed_issue(kernel):
         return None
 
 
+def committed_inst(kernel):
+    """Warp instructions per unit of `kernel` in its committed ncu capture
+    (profiles/traffic.json); None if absent."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return float(json.load(f)[kernel]["warp_inst_per_unit"])
+    except Exception:
+        return None
+
+
+def issue_roofline(kernel, units, launch_ms, clocks):
+    """The instruction-issue roofline of a kernel bound by issue rather than
+    by HBM: its warp instructions per launch (the committed capture's count
+    per unit times the units of a launch) against the GPU's issue rate, one
+    warp instruction per cycle on each of the 4 schedulers of every SM at
+    the SM clock sampled during the run."""
+    per = committed_inst(kernel)
+    if per is None or not launch_ms:
+        return None
+    import torch
+
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    inst = per * units
+    floor_ms = inst / (sms * 4 * mhz * 1e6) * 1e3
+    return {"warp_inst_per_launch": int(inst), "issue_rate_per_s": sms * 4 * mhz * 1e6,
+            "floor_ms": round(floor_ms, 4), "frac": round(floor_ms / launch_ms, 4),
+            "source": "warp instructions per unit of the committed ncu capture "
+                      "(profiles/traffic.json) times the units of a launch"}
+
+
 def committed_traffic(kernel):
     """DRAM bytes per unit (position, or block for the probe decode) of
     `kernel` from profiles/traffic.json, which records one ncu capture of a
@@ -328,6 +359,7 @@ def run_engine(a, rank, world, local):
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "alg_bytes_per_launch": int(alg), "traffic": traffic,
                 "issue_active_frac": committed_issue(dom),
+                "issue": issue_roofline(dom, positions, dom_ms, clk),
                 "step_alg_GBps": round(ALG_BYTES_PER_POS * positions / (ms / 1e3) / 1e9, 1),
                 "step_frac": round(ALG_BYTES_PER_POS * positions / (ms / 1e3) / 1e9 / peak, 4)}
 
@@ -790,6 +822,7 @@ def run_probe(a, rank, world, local):
                 "peak_source": peak_kind, "alg_bytes_per_launch": alg,
                 "traffic": int(tr * touched) if tr else None,
                 "issue_active_frac": committed_issue("k_probe_decode"),
+                "issue": issue_roofline("k_probe_decode", touched, dec_ms, clk),
                 "note": "algorithmic bytes = touched blocks x their tables' mean stream "
                         "bytes per block (each stream read once; the zero padding in front "
                         "of a stream is skipped); the rANS steps, not HBM, bound this kernel"}
