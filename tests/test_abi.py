@@ -74,3 +74,15 @@ def test_tbgen_reports_library_errors_without_gpu():
         pytest.skip("a GPU is present")
     r = subprocess.run([_tbgen(), "KRvK"], capture_output=True, text=True, timeout=120)
     assert r.returncode != 0 and "tbgen: init:" in r.stderr
+
+
+def test_checkers_built_together():
+    """Where the reference-worker harness has been built, the probe harness
+    and the reference's programs have been built beside it (the probe parity
+    tests skip, rather than fail, without them)."""
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    if not os.path.exists(os.path.join(ref, "libtbref.so")):
+        import pytest
+        pytest.skip("reference checkers not built here")
+    for name in ("libtbprobe.so", "tb8gen", "tb8gen_stub"):
+        assert os.path.exists(os.path.join(ref, name)), name
