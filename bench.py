@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="slice",
-                    choices=["slice", "mix", "small", "probe", "serve", "fixpoint"])
+                    choices=["slice", "mix", "small", "slice-pool", "probe", "serve",
+                             "fixpoint"])
     ap.add_argument("--fix-material", default="KQRvKRR")
     ap.add_argument("--fix-max-ply", type=int, default=0)
     ap.add_argument("--serve-jobs", type=int, default=120)
@@ -73,7 +74,7 @@ def parse():
     ap.add_argument("--ctas-per-sm", type=int, default=0,
                     help="persistent-kernel CTAs per SM (0: autotune)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
-                    help="target CPU time of the bounded CPU sample")
+                    help="probe workload: target CPU time of the reference probe sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -91,6 +92,8 @@ def workload_spec(name):
         return [("KRRRvKRRR", 96, 0.01, 1)]
     if name == "small":  # profiling case: 24 MB bitmaps
         return [("KQRRvKRR", 96, 0.01, 1)]
+    if name == "slice-pool":  # profiling case: the slice, neighbours in shared sinks (~1.4 GB)
+        return [("KRRRvKRRR", 96, 0.01, 1)]
     import numpy as np
 
     rng = np.random.default_rng(2)
@@ -242,7 +245,7 @@ def run_engine(a, rank, world, local):
     jobs = []
     for mat, s, p, seed in spec:
         pool = None
-        if a.workload == "mix":
+        if a.workload in ("mix", "slice-pool"):
             if mat not in pools:
                 pools[mat] = MaterialPool(mat, seed)
             pool = pools[mat]
@@ -363,19 +366,21 @@ def run_engine(a, rank, world, local):
                 "step_alg_GBps": round(ALG_BYTES_PER_POS * positions / (ms / 1e3) / 1e9, 1),
                 "step_frac": round(ALG_BYTES_PER_POS * positions / (ms / 1e3) / 1e9 / peak, 4)}
 
-    cpu = None
+    cpu, ref_ply = None, None
     if rank == 0 and world == 1 and not a.no_cpu:
-        cpu = run_cpu_baseline(a, jobs)
+        cpu, ref_ply = run_cpu_baseline(a, jobs)
+    # bit-exactness of the timed step's outputs (outside the timing)
+    parity = slice_parity(jobs, ref_ply)
+    del ref_ply
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded Bernoulli bitmaps, seeded 7-piece stub)",
-        "config": {"workload": a.workload, "path": a.path, "slices": len(jobs),
-                   "positions_per_step": positions,
-                   "materials": sorted({j.material for j in jobs}),
-                   "l2": "inputs larger than L2 (>=16 MB bitmaps, many per step)"},
+        "config": slice_config(a.workload, spec, positions),
+        "path": a.path,
+        "parity": parity,
         "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
         "paths_ms": {"plain": round(plain_ms, 4), "batched": round(batched_ms, 4),
                      "batched_speedup": round(plain_ms / batched_ms, 3)},
@@ -465,7 +470,7 @@ def run_e2e(a, jobs, stream, positions, mode):
 
     run(2)
     torch.cuda.synchronize()
-    steps = max(2, min(a.steps, 5))
+    steps = max(2, a.steps)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -490,13 +495,14 @@ def cpu_oracle(material, nthreads):
     return orc.Port(material), "port"
 
 
-def run_cpu_baseline(a, jobs, budget=None, inputs=None, oracle=None):
-    """The reference's CPU ply (oracle/_ref, all host cores) on a bounded
-    sample of the first job: sources restricted to a leading fraction of
-    the slice, time extrapolated to the whole slice."""
+def run_cpu_baseline(a, jobs, inputs=None, oracle=None):
+    """The reference's CPU ply (oracle/_ref, all host cores) on one whole
+    slice-ply of the first job (no sampling): the W step, the epilogue, the
+    L step and the verify over all N positions of the slice.  Returns the
+    baseline record and the finished CPU ply (its outputs() are compared
+    with the engine's)."""
     from oracle.plyjob_cpu import CpuSlicePly
 
-    budget = budget or a.cpu_seconds
     cores = os.cpu_count() or 1
     job = inputs if inputs is not None else jobs[0]
     material = job["material"] if isinstance(job, dict) else job.material
@@ -506,65 +512,144 @@ def run_cpu_baseline(a, jobs, budget=None, inputs=None, oracle=None):
         O, kind = oracle
     O.set_stub(1, 3)
     threads = getattr(O, "nthreads", 1)
-    frac = 0.002
-    c = CpuSlicePly(O, job, frac)
+    c = CpuSlicePly(O, job, 1.0)
     t = c.step()
-    scal = c.times["w_scatter"] + c.times["l_scatter"] + c.times["l_verify"]
-    fixed = c.times["w_epilogue"]
-    want = max(0.0, budget - fixed)
-    frac2 = min(1.0, max(frac, frac * want / max(scal, 1e-6)))
-    if frac2 > frac * 1.5:
-        c = CpuSlicePly(O, job, frac2)
-        t = c.step()
-        frac = frac2
-        scal = c.times["w_scatter"] + c.times["l_scatter"] + c.times["l_verify"]
-        fixed = c.times["w_epilogue"]
-    t_full = scal / frac + fixed
-    positions = c.N
-    return {"value": round(positions / t_full, 1), "unit": UNIT, "cores": threads,
+    return {"value": round(c.N / t, 1), "unit": UNIT, "cores": threads,
             "kind": kind, "seconds_measured": round(t, 3),
-            "sample": (f"{material} slice {c.s}: scatter sources restricted to the first "
-                       f"{frac:.4f} of the slice, epilogue and verify over the whole slice; "
-                       f"scatter+verify time scaled by 1/{frac:.4f}"),
-            "phase_s": {k: round(v, 4) for k, v in c.times.items()}}
+            "sample": (f"one whole slice-ply of {material} slice {c.s} ({c.N} positions, "
+                       f"no sampling): W step, epilogue, L step and verify"),
+            "phase_s": {k: round(v, 4) for k, v in c.times.items()}}, c
+
+
+GOLDEN_SLICE = os.path.join(ROOT, "tests", "golden", "slice_ply.json")
+
+
+def golden_slice(material, s, p, seed):
+    """The reference's recorded outputs of one slice-ply
+    (tests/golden/slice_ply.json, made by tests/golden/make_slice_golden.py
+    with the reference's workers), or None."""
+    try:
+        with open(GOLDEN_SLICE) as f:
+            return json.load(f).get(f"{material}/{s}/{p}/{seed}")
+    except OSError:
+        return None
+
+
+def compare_outputs(eng: dict, ref: dict) -> list:
+    """Names of the bitmaps that differ between the engine's outputs
+    (device tensors) and the reference's (numpy arrays)."""
+    import numpy as np
+
+    bad = [k for k in sorted(set(eng) | set(ref)) if k not in eng or k not in ref]
+    for k in sorted(set(eng) & set(ref)):
+        if not np.array_equal(eng[k].cpu().numpy(), ref[k]):
+            bad.append(k)
+    return bad
+
+
+def slice_parity(jobs, ref_ply=None):
+    """Bit-exactness of the workload's slice-plies: the digests and counts
+    of the recorded reference outputs where the golden file has the job,
+    and a byte-for-byte comparison with a reference ply run in this process
+    on the same inputs (ref_ply, for the first job)."""
+    from tb8gen_b200.plyjob import output_digests
+
+    out = {"golden": "not recorded", "jobs_checked": 0}
+    bad = []
+    for j in jobs:
+        g = golden_slice(j.material, j.s, j.p, j.seed)
+        if g is None or j.pool is not None:
+            continue
+        counts = list(j.counts())
+        dig = output_digests(j.outputs())
+        out["jobs_checked"] += 1
+        if counts != g["counts"] or dig != g["sha256"]:
+            bad.append(f"{j.material}/{j.s}: counts {counts} vs {g['counts']}, digests differ "
+                       f"in {[k for k in dig if dig[k] != g['sha256'].get(k)]}")
+        if out["jobs_checked"] == 1:
+            out["counts"] = counts
+            out["digests"] = {k: v[:16] for k, v in dig.items()}
+    if out["jobs_checked"]:
+        out["golden"] = "differ" if bad else "equal"
+    if ref_ply is not None:
+        diff = compare_outputs(jobs[0].outputs(), ref_ply.outputs())
+        out["vs_reference"] = "differ" if diff else "equal"
+        out["vs_reference_bitmaps"] = len(ref_ply.outputs())
+        if diff:
+            bad.append(f"{jobs[0].material}/{jobs[0].s} differs from the reference ply in {diff}")
+    out["mismatches"] = bad
+    return out
+
+
+def slice_config(workload, spec, positions):
+    """The `config` of a ply workload, the same dict in both arms."""
+    mats = sorted({m for m, _, _, _ in spec})
+    cfg = {"workload": workload, "slices": len(spec), "materials": mats,
+           "positions_per_step": positions,
+           "p": sorted({p for _, _, p, _ in spec}), "seed": spec[0][3],
+           "l2": "inputs larger than L2 (>=16 MB bitmaps, many per step)"}
+    if len(spec) == 1:
+        cfg["slice"] = spec[0][1]
+    return cfg
 
 
 def run_reference(a, rank, world, local, spec=None):
     """Reference arm: the reference's own CPU workers (oracle/_ref) on all
-    host cores, inputs built on the CPU by the same workers (no engine)."""
+    host cores, inputs built on the CPU by the same workers (no engine).
+    A step is one whole slice-ply of the workload's first slice (for the
+    slice workload, the whole workload); the first step's outputs are
+    checked against the recorded reference digests."""
     if rank != 0:
         return None
-    from oracle.plyjob_cpu import inputs_from_oracle
+    from oracle.plyjob_cpu import CpuSlicePly, inputs_from_oracle
+    from tb8gen_b200.plyjob import output_digests
 
     cores = os.cpu_count() or 1
-    mat, s, p, seed = spec or workload_spec(a.workload)[0]
+    full_spec = [spec] if spec else workload_spec(a.workload)
+    mat, s, p, seed = full_spec[0]
     O, kind = cpu_oracle(mat, cores)
     O.set_stub(1, 3)
     t0 = time.time()
     inputs = inputs_from_oracle(O, mat, s, p, seed)
     prep = time.time() - t0
     per_step = []
-    info = None
-    for _ in range(a.warmup + a.steps):
-        info = run_cpu_baseline(a, None, budget=min(a.cpu_seconds, 20.0), inputs=inputs,
-                                oracle=(O, kind))
-        per_step.append(inputs["N"] / info["value"])
+    parity = {"golden": "not recorded"}
+    ply = CpuSlicePly(O, inputs, 1.0)
+    for i in range(a.warmup + a.steps):
+        per_step.append(ply.step())
+        if i == 0:
+            g = golden_slice(mat, s, p, seed)
+            counts = list(ply.counts())
+            dig = output_digests(ply.outputs())
+            parity = {"counts": counts, "digests": {k: v[:16] for k, v in dig.items()}}
+            if g is not None:
+                parity["golden"] = "equal" if (counts == g["counts"] and dig == g["sha256"]) \
+                    else "differ"
     ts = per_step[a.warmup:] or per_step
     tm = statistics.median(ts)
     v = inputs["N"] / tm
+    threads = getattr(O, "nthreads", 1)
+    cfg = slice_config(a.workload, [(mat, s, p, seed)], inputs["N"])
+    if len(full_spec) > 1:
+        cfg["note"] = (f"the reference arm runs the first of the workload's {len(full_spec)} "
+                       "slices per step")
+    sample = (f"one whole slice-ply of {mat} slice {s} ({inputs['N']} positions, no "
+              f"sampling) per step")
     return {
         "metric": METRIC, "value": round(v, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(tm * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded Bernoulli bitmaps, seeded 7-piece stub)",
-        "config": {"workload": a.workload, "slices": 1, "material": mat, "slice": s,
-                   "note": "first slice of the workload; a step is one slice-ply"},
+        "config": cfg,
         "impl": "reference",
-        "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": info["cores"],
-                         "kind": info["kind"], "sample": info["sample"]},
+        "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": threads,
+                         "kind": kind, "sample": sample},
         "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "parity": parity,
+        "phase_s": {k: round(x, 4) for k, x in ply.times.items()},
         "input_prep_s": round(prep, 1),
+        "seconds_timed": round(sum(ts), 1),
     }
 
 
@@ -932,7 +1017,7 @@ def run_probe_e2e(a, ps, stream, compact=True):
 
     run(2)
     torch.cuda.synchronize()
-    steps = max(2, min(a.steps, 5))
+    steps = max(2, a.steps)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -1168,8 +1253,8 @@ def run_fixpoint(a, rank, world, local):
 
         O, kind = cpu_oracle(mat, os.cpu_count() or 1)
         O.set_stub(1, 3)
-        cpu = run_cpu_baseline(a, None, budget=min(a.cpu_seconds, 15.0),
-                               inputs=inputs_from_oracle(O, mat, 96, 0.01, 1), oracle=(O, kind))
+        cpu, _ = run_cpu_baseline(a, None, inputs=inputs_from_oracle(O, mat, 96, 0.01, 1),
+                                  oracle=(O, kind))
     plies = stats.get("plies", 0)
     return {
         "metric": FIX_METRIC, "value": round(value, 1), "unit": "positions/s", "n_gpus": world,
@@ -1241,6 +1326,11 @@ def main():
             line = run_engine(a, rank, world, local)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
+            par = line.get("parity") or {}
+            if "differ" in (par.get("golden"), par.get("vs_reference")):
+                sys.stderr.write("bench: outputs differ from the reference: "
+                                 f"{par.get('mismatches')}\n")
+                sys.exit(1)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -102,7 +102,11 @@ int tbg_set_stream(void *stream);
 int tbg_set_stub(uint64_t seed, int modulus);
 
 /* Device memory for a C host that binds its own slices (kslice_setup's
- * alloc_huge, kslice.c:198-227): zero-filled, 256-byte aligned. */
+ * alloc_huge, kslice.c:198-227): zero-filled, 256-byte aligned.
+ * TBG_ERR_NOMEM when the device cannot hold it, where the reference exits
+ * (out_of_mem, util.c:111-115).  For tests of that path, the environment
+ * variable TBG_FAIL_ALLOC_AT=k (read by tbg_init) makes the k-th call of
+ * tbg_alloc / tbg_host_alloc in the process fail that way. */
 int tbg_alloc(size_t bytes, void **dev);
 int tbg_free(void *dev);
 

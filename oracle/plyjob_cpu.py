@@ -139,3 +139,19 @@ class CpuSlicePly:
         self.times = {"w_scatter": t1 - t0, "w_epilogue": t2 - t1,
                       "l_scatter": t3 - t2, "l_verify": t4 - t3}
         return t4 - t0
+
+    def outputs(self) -> dict:
+        """Every bitmap a step writes, named as tb8gen_b200.plyjob.SlicePly
+        .outputs() names them: W(s), wins(s), L(s) and the king-move marks
+        into the neighbour slices (T(t) of white's, X(t) of black's)."""
+        out = {"W(s)": self.T, "wins(s)": self.wins, "L(s)": self.X}
+        if not self.shared:
+            for t, b in self.T_nbr.items():
+                out[f"T({t})"] = b
+            for t, b in self.X_nbr.items():
+                out[f"X({t})"] = b
+        return out
+
+    def counts(self):
+        """(|W(s)|, |L(s)|) after a step."""
+        return self.O.count(self.T), self.O.count(self.X)

@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 
@@ -219,8 +220,14 @@ int Engine::add_material(const int *pt, int num) {
 static const int kOrder[16] = {0, 0, 3, 5, 7, 9, 1, 0, 0, 0, 4, 6, 8, 10, 2, 0};
 
 // -------------------------------------------------------------- launches
+bool Engine::alloc_refused() {
+  alloc_calls++;
+  return fail_alloc_at > 0 && alloc_calls == fail_alloc_at;
+}
+
 int Engine::ensure_device() {
   if (dev_ready) return TBG_OK;
+  if (const char *v = getenv("TBG_FAIL_ALLOC_AT")) fail_alloc_at = strtol(v, nullptr, 10);
   CK(cudaGetDevice(&device));
   CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
   CK(cudaMalloc(&d_status, sizeof(DevStatus)));
@@ -1087,6 +1094,9 @@ extern "C" int tbg_alloc(size_t bytes, void **dev) {
   if (!dev || bytes == 0) return fail(TBG_ERR_ARG, "bad allocation request");
   if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
   *dev = nullptr;
+  if (g_eng.alloc_refused())
+    return fail(TBG_ERR_NOMEM, "cudaMalloc(%zu): allocation %ld refused (TBG_FAIL_ALLOC_AT)",
+                bytes, g_eng.alloc_calls);
   cudaError_t e = cudaMalloc(dev, bytes);
   if (e != cudaSuccess) return fail(TBG_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
   // Zeroed on a stream of its own and waited for: a plain cudaMemset would
@@ -1206,6 +1216,9 @@ extern "C" int tbg_host_alloc(size_t bytes, void **host) {
   if (!host || bytes == 0) return fail(TBG_ERR_ARG, "bad allocation request");
   if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
   *host = nullptr;
+  if (g_eng.alloc_refused())
+    return fail(TBG_ERR_NOMEM, "cudaHostAlloc(%zu): allocation %ld refused (TBG_FAIL_ALLOC_AT)",
+                bytes, g_eng.alloc_calls);
   cudaError_t e = cudaHostAlloc(host, bytes, cudaHostAllocDefault);
   if (e != cudaSuccess) {
     cudaGetLastError();

@@ -106,8 +106,14 @@ struct Engine {
   cudaStream_t s_zero = nullptr;  // zero-fills new allocations (tbg_alloc)
   std::vector<cudaEvent_t> tick_ev;
   uint64_t next_ticket = 1;
+  // Host-side failure injection: TBG_FAIL_ALLOC_AT=k (read at tbg_init)
+  // makes the k-th allocation through tbg_alloc / tbg_host_alloc fail with
+  // TBG_ERR_NOMEM, as a failed cudaMalloc or cudaHostAlloc would.
+  long fail_alloc_at = 0;
+  long alloc_calls = 0;
 
   int ensure_device();
+  bool alloc_refused();
   int add_material(const int *pt, int num);
   int fill_job(SliceJob &J, int stm, int s, bool need_sub);
   int grid_for(uint64_t units, int per_sm);

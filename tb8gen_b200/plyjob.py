@@ -253,6 +253,18 @@ class SlicePly:
         self.l_scatter()
         self.l_verify()
 
+    def outputs(self) -> dict:
+        """Every bitmap a step writes (device tensors): W(s), the new
+        wins(s), L(s) and, with per-neighbour buffers, the king-move marks
+        into the neighbour slices (T(t) for white's, X(t) for black's)."""
+        out = {"W(s)": self.T, "wins(s)": self.wins, "L(s)": self.X}
+        if self.pool is None:
+            for t, b in self.T_nbr.items():
+                out[f"T({t})"] = b
+            for t, b in self.X_nbr.items():
+                out[f"X({t})"] = b
+        return out
+
     def counts(self):
         """(|W(s)|, |L(s)|) after a step."""
         self.m.select()
@@ -260,6 +272,23 @@ class SlicePly:
         tbg.bind(0, self.T)
         tbg.bind(1, self.X)
         return tbg.count(0), tbg.count(1)
+
+
+def bitmap_digest(a) -> str:
+    """SHA-256 of a bitmap's bytes (a numpy array or a tensor, any device)."""
+    import hashlib
+
+    import numpy as np
+
+    if isinstance(a, torch.Tensor):
+        a = a.detach().contiguous().cpu().numpy()
+    return hashlib.sha256(np.ascontiguousarray(a).view(np.uint8).tobytes()).hexdigest()
+
+
+def output_digests(outputs: dict) -> dict:
+    """{name: SHA-256} of the bitmaps of SlicePly.outputs() (or of the CPU
+    twin's outputs()), names sorted."""
+    return {k: bitmap_digest(outputs[k]) for k in sorted(outputs)}
 
 
 def record_step(jobs):

@@ -186,12 +186,22 @@ class _Job:
     out: list | None = None
 
 
+class SpillError(RuntimeError):
+    """The pinned host tier cannot take a spilled slice state (its budget
+    is spent, or the host refused to lock more memory)."""
+
+
 class GpuExecutor:
-    """Runs requests through the C ABI, one CUDA stream per slot."""
+    """Runs requests through the C ABI, one CUDA stream per slot.
+
+    `host_budget_bytes` caps the page-locked host memory that spilled slice
+    states may hold (None: whatever the host grants); a spill beyond it
+    raises SpillError instead of admitting the request, as the reference
+    exits when its disk tier fails (util.c:229-243)."""
 
     def __init__(self, ply_materials, tables: dict, pools: dict, slots: int,
                  budget_bytes: int, keep_results: bool = False, probe_max: int = 1_000_000,
-                 query_bytes: int = 16):
+                 query_bytes: int = 16, host_budget_bytes: int | None = None):
         import torch
 
         import tb8gen_b200 as tbg
@@ -223,6 +233,8 @@ class GpuExecutor:
             self.used += self.probe_scratch[m]
         self.states = collections.OrderedDict()     # (material, slice) -> _State
         self.spills = 0
+        self.host_budget = host_budget_bytes
+        self.host_used = 0
         self.reloads = 0
         self.builds = 0
         self.peak = self.used
@@ -261,10 +273,24 @@ class GpuExecutor:
             self._spill(st)
         return self.used + need <= self.budget
 
+    def _host_tier(self, sizes):
+        """Page-locked host buffers for a spilled state, within the host
+        budget; SpillError when they do not fit or cannot be locked."""
+        need = sum(sizes)
+        if self.host_budget is not None and self.host_used + need > self.host_budget:
+            raise SpillError(f"pinned host tier full: {self.host_used} + {need} bytes > "
+                             f"budget {self.host_budget}")
+        try:
+            bufs = [self.torch.empty(n, dtype=self.torch.uint8, pin_memory=True) for n in sizes]
+        except RuntimeError as e:
+            raise SpillError(f"cannot lock {need} bytes of host memory: {e}") from e
+        self.host_used += need
+        return bufs
+
     def _spill(self, st):
         torch = self.torch
         if st.host is None:
-            st.host = [torch.empty(b.numel(), dtype=torch.uint8, pin_memory=True) for b in st.dev]
+            st.host = self._host_tier([b.numel() for b in st.dev])
         with torch.cuda.stream(self.spill_stream):
             if st.ready is not None:
                 self.spill_stream.wait_event(st.ready)
