@@ -77,6 +77,8 @@ def parse():
                     help="probe workload: target CPU time of the reference probe sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mix", action="store_true",
+                    help="slice workload: skip the uneven-mix record (batched vs plain)")
     return ap.parse_args()
 
 
@@ -275,28 +277,11 @@ def run_engine(a, rank, world, local):
     mode = 1 if a.path == "batched" else 0
 
     def time_mode(md, reps):
-        tbg.batch_run(md)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            tbg.batch_run(md)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
+        return time_batch(tbg, stream, md, reps)
 
-    # autotune the persistent launch (CTAs per SM) on this batch
-    tune = {}
-    if a.ctas_per_sm > 0:
-        tbg.batch_tune(a.ctas_per_sm)
-        best_cps = a.ctas_per_sm
-    else:
-        for cps in (1, 2, 3, 4):
-            tbg.batch_tune(cps)
-            tune[cps] = round(time_mode(1, 2), 4)
-        best_cps = min(tune, key=tune.get)
-        tbg.batch_tune(best_cps)
+    # autotune the persistent launch on this batch: CTAs per SM x tiles per
+    # scatter work item
+    tune, best_cps, best_gt, nitems = autotune(tbg, time_mode, a.ctas_per_sm)
 
     def step():
         tbg.batch_run(mode)
@@ -337,6 +322,10 @@ def run_engine(a, rank, world, local):
                 for ph in phase_names}
 
     counts = [j.counts() for j in jobs[:4]]
+    mix = None
+    if a.workload == "slice" and not a.no_mix:
+        mix = mix_record(a, stream)
+        tbg.batch_shape(best_gt)  # the timed batch's shape for what follows
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -385,12 +374,109 @@ def run_engine(a, rank, world, local):
         "paths_ms": {"plain": round(plain_ms, 4), "batched": round(batched_ms, 4),
                      "batched_speedup": round(plain_ms / batched_ms, 3)},
         "batch": {"calls": nops, "work_items": nitems, "ctas_per_sm": best_cps,
-                  "autotune_ms": tune},
+                  "scatter_tiles": best_gt, "autotune_ms": tune},
         "counts_first_jobs": counts,
         "roofline": roofline, "gpu_launches": launches, "clocks": clk,
         "e2e": e2e, "cpu_baseline": cpu,
+        "mix": mix,
     }
     return line
+
+
+def time_batch(tbg, stream, md, reps):
+    """Device time (ms) of one run of the selected recorded batch: mode 0
+    one launch per call, mode 1 the persistent launch."""
+    import torch
+
+    tbg.batch_run(md)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        tbg.batch_run(md)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+TUNE_CPS = (2, 3, 4)
+TUNE_SCATTER_TILES = (1, 2, 4)
+
+
+def autotune(tbg, time_mode, fixed_cps=0):
+    """The persistent launch's shape picked on the recorded batch by its own
+    device time: CTAs per SM (the blocks that take work items at once) x
+    tiles per scatter work item (the sources a block gathers before handing
+    them out).  Returns ({"<cps>x<tiles>": ms}, cps, tiles, work items)."""
+    tune = {}
+    for gt in TUNE_SCATTER_TILES:
+        tbg.batch_shape(gt)
+        for cps in ((fixed_cps,) if fixed_cps > 0 else TUNE_CPS):
+            tbg.batch_tune(cps)
+            tune[f"{cps}x{gt}"] = round(time_mode(1, 2), 4)
+    best = min(tune, key=tune.get)
+    cps, gt = (int(x) for x in best.split("x"))
+    nitems = tbg.batch_shape(gt)
+    tbg.batch_tune(cps)
+    return tune, cps, gt, nitems
+
+
+def mix_record(a, stream, slot=2):
+    """The uneven mix (96 slices of three materials, seed 2) recorded in its
+    own batch slot beside the timed workload: the persistent launch against
+    one launch per call, each autotuned on the batch, and every slice's
+    W and L counts and digests checked against the reference's recorded
+    ones (tests/golden/slice_ply.json "mix", made by the reference's
+    workers)."""
+    import torch
+
+    import tb8gen_b200 as tbg
+    from tb8gen_b200.plyjob import MaterialPool, SlicePly, output_digests, record_step
+
+    spec = workload_spec("mix")
+    pools, jobs = {}, []
+    for mat, s, p, seed in spec:
+        if mat not in pools:
+            pools[mat] = MaterialPool(mat, seed)
+        jobs.append(SlicePly(mat, s, p, seed, pools[mat]))
+    positions = sum(j.positions for j in jobs)
+    tbg.batch_select(slot)
+    try:
+        nops, _ = record_step(jobs)
+        tm = lambda md, reps: time_batch(tbg, stream, md, reps)
+        tune, cps, gt, nitems = autotune(tbg, tm)
+        reps = max(2, min(a.steps, 5))
+        plain = tm(0, reps)
+        batched = tm(1, reps)
+        tbg.sync()
+    finally:
+        tbg.batch_select(0)
+    golden = {}
+    try:
+        with open(GOLDEN_SLICE) as f:
+            golden = json.load(f).get("mix", {})
+    except OSError:
+        pass
+    checked, bad = 0, []
+    for j in jobs:
+        g = golden.get(f"{j.material}/{j.s}/{j.p}/{j.seed}/shared")
+        if g is None:
+            continue
+        checked += 1
+        if list(j.counts()) != g["counts"] or output_digests(j.outputs()) != g["sha256"]:
+            bad.append(f"{j.material}/{j.s}/{j.p}")
+    rec = {"slices": len(jobs), "positions_per_step": positions,
+           "materials": sorted(pools), "plain_ms": round(plain, 3),
+           "batched_ms": round(batched, 3), "batched_speedup": round(plain / batched, 3),
+           "value_batched": round(positions / (batched / 1e3), 1),
+           "calls": nops, "work_items": nitems, "ctas_per_sm": cps, "scatter_tiles": gt,
+           "autotune_ms": tune,
+           "parity": {"golden": ("differ" if bad else "equal") if checked else "not recorded",
+                      "slices_checked": checked, "mismatches": bad}}
+    del jobs, pools
+    torch.cuda.empty_cache()
+    return rec
 
 
 def run_e2e(a, jobs, stream, positions, mode):
@@ -1209,6 +1295,25 @@ def parse_tbgen(stderr):
     return times, stats
 
 
+def fixpoint_parity(material, counts):
+    """The generation's count lines against the reference program's run of
+    the same material and stub (tests/golden/fixpoint_<material>.json, made
+    by tests/golden/make_fixpoint_golden.py from the reference's whole
+    generation): every line, or the leading lines of a generation cut short
+    by --fix-max-ply."""
+    path = os.path.join(ROOT, "tests", "golden", f"fixpoint_{material}.json")
+    if not os.path.exists(path):
+        return {"vs_reference": "not recorded"}
+    with open(path) as f:
+        ref = json.load(f)["counts"]
+    mine = [c for c in counts if not c.startswith("sum ")]
+    n = min(len(mine), len(ref))
+    same = n > 0 and mine[:n] == ref[:n] and len(mine) <= len(ref)
+    return {"vs_reference": "equal" if same else "differ", "count_lines_compared": n,
+            "reference_lines": len(ref),
+            "source": "the reference program's whole generation (tb8gen_stub, stub seed 1 mod 3)"}
+
+
 def run_fixpoint(a, rank, world, local):
     """The whole generation of one material (calc_sub, illegal and mate,
     then calc_L_n / calc_W_n until no bitmap changes) by the C host driver
@@ -1270,6 +1375,7 @@ def run_fixpoint(a, rank, world, local):
         "total_s": round(wall, 2), "half_ply_ms_total": round(ms, 1),
         "resident_half_ply_ms_total": round(sum(t for _, t, _ in t2), 1),
         "counts_match_resident": counts == counts2 and r2.returncode == 0,
+        "parity": fixpoint_parity(mat, counts),
         "count_lines": len(counts), "last_counts": counts[-4:],
         "slice_digests_compared": sum(1 for c in counts if c.startswith("sum ")),
         "slices_per_digest": 16,
@@ -1327,7 +1433,8 @@ def main():
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
             par = line.get("parity") or {}
-            if "differ" in (par.get("golden"), par.get("vs_reference")):
+            mixpar = ((line.get("mix") or {}).get("parity") or {}).get("golden")
+            if "differ" in (par.get("golden"), par.get("vs_reference"), mixpar):
                 sys.stderr.write("bench: outputs differ from the reference: "
                                  f"{par.get('mismatches')}\n")
                 sys.exit(1)

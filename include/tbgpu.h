@@ -180,6 +180,17 @@ int tbg_unbind_all(void);
  * into slice s and the slices its king moves reach (all must be bound). */
 int tbg_predecessors(int stm, int s);
 
+/* The candidates phase of calc_L_n (tb8gen.c:951-997) for a host that
+ * verifies them next against the same "wins": predecessors(stm, s) where
+ * a predecessor that a quiet move of the unmoved slider (one square along
+ * its ray) takes to a position outside the opponent's "wins" of slice s
+ * (opp_wins, bytes >= the slice bitmap) is not marked in slice s -- it
+ * cannot survive check_successors (check_moves, tb8gen.c:594-602).  The
+ * verified losses are the reference's; the candidates are a subset of
+ * predecessors()'s.  No counterpart in the reference: it marks every
+ * predecessor and verifies all of them. */
+int tbg_candidates(int stm, int s, const void *opp_wins, size_t bytes);
+
 /* predecessors_sub(stm, s, legality), tb8gen.c:397-414: uncaptures from
  * the sub buffer bound to s (sets of colour stm^1) into slice s and its
  * king-move slices. */
@@ -280,6 +291,15 @@ int tbg_batch_counts_async(uint64_t *host_out, int n);
  * a batch is being recorded. */
 int tbg_batch_select(int slot);
 
+/* Work-item shape of scatters (tiles of 32,768 positions per item of the
+ * persistent queue and per block of a plain launch; 0: one tile): a block
+ * gathers the sources of an item's tiles before handing them out to its
+ * threads.  Applies to later recordings and re-cuts the selected recorded
+ * batch (*nitems: its work items now, 0 if none is recorded; nitems may be
+ * NULL).  Results do not depend on it.  No counterpart in the reference
+ * (its g_total_work ranges, tb8gen.c:1327, are the nearest knob). */
+int tbg_batch_shape(int scatter_tiles, uint64_t *nitems);
+
 /* Persistent-launch configuration of every slot: CTAs per SM (default 4),
  * and the iteration bound of a dependency wait (<= 0 keeps the current
  * one). */
@@ -312,8 +332,10 @@ int tbg_launches(uint64_t *n);
  * wins_in may equal wins_out.  `bytes` (a multiple of 16) is the bitmap size;
  * at most 1 GiB (TBG_ERR_RANGE beyond).  The first call on a device looks up
  * the scratch address on that device; make it before any stream capture.
- * Calls share the scratch: calls that overlap on the GPU race and must not
- * be issued.  Waits for the stream before returning the count. */
+ * The address is kept for the life of the device's primary context (not
+ * valid after a cudaDeviceReset).  Calls share the scratch: calls that
+ * overlap on the GPU race and must not be issued.  Waits for the stream
+ * before returning the count. */
 int tbg_epilogue_W_static(void *dev_T, const void *dev_wins_in, void *dev_wins_out,
                           uint64_t nbits, uint64_t bytes, void *stream,
                           uint64_t *cnt);

@@ -46,11 +46,14 @@ def inputs_from_engine_job(job) -> dict:
     return d
 
 
-def inputs_from_oracle(O, material: str, s: int, p: float, seed: int) -> dict:
+def inputs_from_oracle(O, material: str, s: int, p: float, seed: int,
+                       shared: bool = False) -> dict:
     """The same inputs as tb8gen_b200.plyjob.SlicePly(material, s, p, seed)
-    (no shared neighbours), computed on the CPU by the oracle O itself: the
-    illegal masks and sub/win bitmaps by its calc_illegal / calc_sub, the
-    Bernoulli sources by the same seeded splitmix64 stream."""
+    computed on the CPU by the oracle O itself: the illegal masks and
+    sub/win bitmaps by its calc_illegal / calc_sub, the Bernoulli sources by
+    the same seeded splitmix64 stream.  With `shared`, the neighbours are
+    those of a MaterialPool: one "wins" (white's illegal mask of slice 0) and
+    one sub/win (of slice 0) for every neighbour, marks into shared sinks."""
     from oracle.oracle import bitmap_tag, gen_bitmap, king_targets
 
     N, B = O.size, O.bytes
@@ -71,6 +74,12 @@ def inputs_from_oracle(O, material: str, s: int, p: float, seed: int) -> dict:
          "W_prev": gen_bitmap(N, B, seed, bitmap_tag(3, WHITE, s), p) & ~ill_w,
          "wins_in": ill_w, "sub_win": sub_win(s),
          "wk": king_targets(WHITE, s), "bk": king_targets(BLACK, s), "shared": False}
+    if shared:
+        d["shared"] = True
+        d["pool_wins"], d["pool_sub"] = illegal(0)[0], sub_win(0)
+        d["wins_nbr"] = {t: None for t in d["bk"]}
+        d["sub_nbr"] = {t: None for t in d["bk"]}
+        return d
     d["wins_nbr"] = {t: illegal(t)[0] for t in d["bk"]}
     d["sub_nbr"] = {t: sub_win(t) for t in d["bk"]}
     return d

@@ -53,6 +53,7 @@ def lib():
             "tbg_sub_bind": [i, vp, sz],
             "tbg_unbind_all": [],
             "tbg_predecessors": [i, i],
+            "tbg_candidates": [i, i, vp, sz],
             "tbg_predecessors_sub": [i, i, i],
             "tbg_check_successors": [i, i],
             "tbg_calc_sub": [i, i, vp * 5],
@@ -74,6 +75,7 @@ def lib():
             "tbg_batch_run": [i],
             "tbg_batch_counts": [C.POINTER(u64), i],
             "tbg_batch_tune": [i, C.c_longlong],
+            "tbg_batch_shape": [i, C.POINTER(u64)],
             "tbg_batch_select": [i],
             "tbg_batch_count": [i],
             "tbg_mark": [C.POINTER(u64)],
@@ -178,6 +180,13 @@ def predecessors(stm: int, s: int):
 
 def predecessors_sub(stm: int, s: int, legality: bool):
     check(lib().tbg_predecessors_sub(stm, s, int(bool(legality))))
+
+
+def candidates(stm: int, s: int, opp_wins):
+    """predecessors(stm, s) without the predecessors that a one-square slider
+    step takes out of opp_wins (the opponent's "wins" of slice s), for an L
+    step that verifies against the same opp_wins next."""
+    check(lib().tbg_candidates(stm, s, ptr(opp_wins), opp_wins.numel() * opp_wins.element_size()))
 
 
 def check_successors(stm: int, s: int):
@@ -290,6 +299,14 @@ def batch_counts(n: int):
 
 def batch_tune(ctas_per_sm: int, spin_limit: int = 0):
     check(lib().tbg_batch_tune(ctas_per_sm, spin_limit))
+
+
+def batch_shape(scatter_tiles: int = 0) -> int:
+    """Tiles per scatter work item (0: one); re-cuts the selected recorded
+    batch and returns its work items (0 if none is recorded)."""
+    n = C.c_uint64()
+    check(lib().tbg_batch_shape(scatter_tiles, C.byref(n)))
+    return n.value
 
 
 def batch_count(s: int):

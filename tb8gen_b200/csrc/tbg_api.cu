@@ -505,9 +505,19 @@ extern "C" int tbg_unbind_all(void) {
 // ---------------------------------------------------------------- ops
 // Every call of the ply step becomes an Op; outside a recording it is
 // launched at once, inside one it is appended to the batch.
-static uint32_t op_tiles(const Op &o) {
+// Work items of an op: 1 MiB chunks of a streaming op, tiles of a verify
+// or an uncapture, groups of gt tiles of a scatter (tbg_batch_shape; one
+// tile unless set): a scatter's block gathers the sparse sources of an
+// item's tiles before handing them out.
+static uint32_t op_tiles(Op &o) {
+  o.gt = 1;
   if (op_streams(o.kind)) return (uint32_t)((o.n16 + kChunk16 - 1) / kChunk16);
-  return (uint32_t)((o.J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull));
+  const uint64_t tiles = (o.J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull);
+  if (o.kind == OP_SCATTER) {
+    const uint64_t g = g_eng.scatter_tiles > 0 ? (uint64_t)g_eng.scatter_tiles : 1;
+    o.gt = (int)std::min<uint64_t>(std::max<uint64_t>(g, 1), std::max<uint64_t>(tiles, 1));
+  }
+  return (uint32_t)((tiles + o.gt - 1) / o.gt);
 }
 
 static int launch_op(const Op &o) {
@@ -515,9 +525,9 @@ static int launch_op(const Op &o) {
   cudaStream_t st = g_eng.stream;
   switch (o.kind) {
   case OP_SCATTER: {
-    const int sp = g_eng.split_for(o.ntiles, g_eng.bps_scatter);
+    const int sp = o.gt > 1 ? 1 : g_eng.split_for(o.ntiles, g_eng.bps_scatter);
     NS_SWITCH(ns, k_predecessors<NS><<<g_eng.grid_for((uint64_t)o.ntiles * sp, g_eng.bps_scatter),
-                                       kThreads, 0, st>>>(o.J, g_eng.d_status, sp));
+                                       kThreads, 0, st>>>(o.J, g_eng.d_status, sp, o.gt));
     return g_eng.check_launch("k_predecessors");
   }
   case OP_SCATTER_SUB: {
@@ -576,6 +586,24 @@ extern "C" int tbg_predecessors(int stm, int s) {
   o.J.src = reinterpret_cast<const uint32_t *>(m.slot[0]);
   o.J.cand = nullptr;
   o.J.nbits = m.d.ii.size;
+  return submit(o);
+}
+
+extern "C" int tbg_candidates(int stm, int s, const void *opp_wins, size_t bytes) {
+  NEED_MAT();
+  if ((stm & ~1) || s < 0 || s >= TBG_NSLICES) return fail(TBG_ERR_ARG, "bad stm/slice");
+  Material &m = g_eng.mats[g_eng.cur];
+  if (!opp_wins || !aligned16(opp_wins) || bytes < m.d.bytes)
+    return fail(TBG_ERR_ARG, "opponent wins of slice %d: need %llu bytes, 16-B aligned", s,
+                (unsigned long long)m.d.bytes);
+  Op o = new_op(OP_SCATTER);
+  int rc = g_eng.fill_job(o.J, stm, s, false);
+  if (rc) return rc;
+  if (!m.slot[0]) return fail(TBG_ERR_UNBOUND, "scratch slot not bound");
+  o.J.src = reinterpret_cast<const uint32_t *>(m.slot[0]);
+  o.J.cand = nullptr;
+  o.J.nbits = m.d.ii.size;
+  o.J.filter = static_cast<const uint32_t *>(opp_wins);
   return submit(o);
 }
 
@@ -886,6 +914,7 @@ static void access_of(const Op &o, Batch::Access &a) {
   switch (o.kind) {
   case OP_SCATTER:
     a.rd.push_back(J.src);
+    if (J.filter) a.rd.push_back(J.filter);
     a.wacc.push_back(J.self);
     for (int d = 0; d < J.nk; d++) a.wacc.push_back(J.kd[d].bits);
     break;
@@ -1035,6 +1064,25 @@ extern "C" int tbg_batch_select(int slot) {
     if (b.recording) return fail(TBG_ERR_STATE, "a batch is being recorded");
   g_eng.bslot = slot;
   return TBG_OK;
+}
+
+extern "C" int tbg_batch_shape(int scatter_tiles, uint64_t *nitems) {
+  if (scatter_tiles < 0 || scatter_tiles > 64) return fail(TBG_ERR_ARG, "scatter_tiles 0..64");
+  for (const Batch &b : g_eng.batches)
+    if (b.recording) return fail(TBG_ERR_STATE, "a batch is being recorded");
+  g_eng.scatter_tiles = scatter_tiles;
+  Batch &b = g_eng.batch();
+  if (nitems) *nitems = 0;
+  if (!b.ready) return TBG_OK;
+  // re-cut the selected batch's work items and upload its queue again
+  b.total = 0;
+  for (Op &o : b.ops) {
+    o.ntiles = op_tiles(o);
+    o.first = b.total;
+    b.total += o.ntiles;
+  }
+  if (nitems) *nitems = b.total;
+  return b.finish();
 }
 
 extern "C" int tbg_batch_tune(int ctas_per_sm, long long spin_limit) {

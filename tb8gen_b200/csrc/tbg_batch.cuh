@@ -71,7 +71,11 @@ template <int NS>
 __device__ __forceinline__ void tile_sparse(const Op &o, SparseSmem &S, uint64_t t,
                                             DevStatus *st) {
   switch (o.kind) {
-  case OP_SCATTER: tile_predecessors<NS>(o.J, S, t, st); break;
+  case OP_SCATTER: {
+    const uint64_t t0 = t * o.gt, tiles = tiles_of(o.J.nbits);
+    tile_predecessors<NS>(o.J, S, t0, (int)min((uint64_t)o.gt, tiles - t0), st);
+    break;
+  }
   case OP_SCATTER_SUB: tile_predecessors_sub<NS>(o.J, S, t, st); break;
   default: tile_check<NS>(o.J, S, t, st, o.out, o.out_words); break;
   }

@@ -94,6 +94,7 @@ struct Engine {
   int bps_scatter = 8;    // grid = SMs x this for the sparse kernels (tiles loop)
   int bps_verify = 8;
   int max_split = 64;     // parts per tile for small bitmaps (tbg_tune_split)
+  int scatter_tiles = 0;  // tiles per scatter work item (tbg_batch_shape; 0: one)
   // Recorded batches: kBatchSlots slots, one selected (tbg_batch_select).
   static constexpr int kBatchSlots = 4;
   Batch batches[kBatchSlots];

@@ -199,7 +199,11 @@ __device__ __forceinline__ void mark(uint32_t *bits, uint64_t idx, uint64_t n, D
     report(st, 1, 2, idx);
     return;
   }
-  atomicOr(bits + (idx >> 5), 1u << (idx & 31));
+  // a fire-and-forget reduction (RED): the old value is never needed
+  asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(
+                   __cvta_generic_to_global(bits + (idx >> 5))),
+               "r"(1u << (idx & 31))
+               : "memory");
 }
 
 __device__ __forceinline__ bool test(const uint32_t *bits, uint64_t idx, uint64_t n,
@@ -578,6 +582,261 @@ __device__ __forceinline__ void mark_piece_unmoves(const SliceJob &J, const DMat
   }
 }
 
+// ------------------------------------------------ incremental index updates
+// A move changes few terms of the index (sq_to_idx_helper, tb8gen.c:129-149:
+// per set, the sum over its squares in increasing order of C(r, i + 1), r
+// the square's rank among the squares not taken by the kings and earlier
+// sets).  The scatter updates the source's index by those terms instead of
+// ranking the target position afresh.
+
+// Rank of square q among the squares not in occ.
+__device__ __forceinline__ int free_rank(int q, bb occ) {
+  return q - __popcll(occ & (bit(q) - 1));
+}
+
+// Index change, over the sets j >= j0, when a king or a piece of a set
+// below j0 moves from a to b: a square q of set j strictly between a and b
+// has one occupied square more or fewer below it, so its rank r moves by
+// one and its term C(r, i + 1) by C(r, i) (upward move) or by -C(r - 1, i)
+// (downward), Pascal's rule, i being q's place in its set; no other term
+// changes.  `kings`: the king squares before the move.
+template <int NS>
+__device__ __forceinline__ uint64_t cross_delta(const DIdx &X, const uint32_t *bin,
+                                                const bb *set, bb kings, int j0, int a, int b) {
+  const bb betw = between(a, b);
+  const bool up = a < b;
+  bb occ = kings;
+  uint64_t d = 0;
+#pragma unroll
+  for (int j = 0; j < NS; j++) {
+    if (j >= j0) {
+      bb c = set[j] & betw;
+      while (c) {
+        const int q = pop_lsb(c);
+        const bb below = bit(q) - 1;
+        const int r = q - __popcll(occ & below);
+        const int i = __popcll(set[j] & below);
+        const uint64_t v = (uint64_t)(up ? bin[i * 64 + r] : bin[i * 64 + r - 1]) * X.factor[j];
+        d = up ? d + v : d - v;
+      }
+    }
+    occ |= set[j];
+  }
+  return d;
+}
+
+// One piece of a set of at most 4 about to move: its set's rank after the
+// move to a square of rank rto with `pos` of the set's other pieces below
+// it is C(rto, pos + 1) + g[pos], where, with the others' ranks o_0 < o_1
+// < ..., g[pos] = sum_{i < pos} C(o_i, i + 1) + sum_{i >= pos} C(o_i, i + 2)
+// (the others below the destination keep their places, those above move
+// up one).
+struct Mover {
+  bb others;
+  uint32_t g[4];
+};
+
+__device__ __forceinline__ void mover_init(Mover &mv, const uint32_t *bin, bb setk, int x,
+                                           bb occk) {
+  mv.others = setk & ~bit(x);
+  uint32_t a[3], b[3];
+  bb o = mv.others;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    a[i] = b[i] = 0;
+    if (o) {
+      const int r = free_rank(pop_lsb(o), occk);
+      a[i] = bin[(i + 1) * 64 + r];
+      b[i] = bin[(i + 2) * 64 + r];
+    }
+  }
+  mv.g[0] = b[0] + b[1] + b[2];
+  mv.g[1] = a[0] + b[1] + b[2];
+  mv.g[2] = a[0] + a[1] + b[2];
+  mv.g[3] = a[0] + a[1] + a[2];
+}
+
+__device__ __forceinline__ uint32_t mover_rank(const Mover &mv, const uint32_t *bin, int to,
+                                               bb occk) {
+  const bb below = bit(to) - 1;
+  const int pos = __popcll(mv.others & below);
+  const int rto = to - __popcll(occk & below);
+  uint32_t g = mv.g[0];
+#pragma unroll
+  for (int p = 1; p < 4; p++)
+    if (pos == p) g = mv.g[p];
+  return bin[(pos + 1) * 64 + rto] + g;
+}
+
+// predecessors_worker's unmoves of one source position (mark_king_unmoves
+// and mark_unmoves, tb8gen.c:246-276) with the targets' indices updated
+// from the source's index idx: a king step without a normalising
+// transform changes only the terms of the squares it passes over; a piece
+// step changes its own set's rank (mover_rank) and the terms of the later
+// sets' squares it passes over.  Sets of more than 4 pieces, and king steps
+// into a transformed slice, are ranked afresh.
+//
+// With J.filter (the opponent's "wins" of slice s, tbg_candidates) the
+// sliders' unmoves into slice s are filtered: a predecessor P whose piece
+// stands on the ray from x at t_k can step to the ray's next square toward
+// x (t_{k-1}), or, at t_1, away from it (t_2); both squares are empty, and
+// the position reached is the one the unmove to that square gives.  If
+// that position is not in the opponent's "wins", P has a quiet move out of
+// them and cannot be lost (check_moves, tb8gen.c:594-602): it is not
+// marked.  A ray of one square, knights and king unmoves are marked as
+// before.
+template <int NS>
+__device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDest *kd,
+                                                 const DMat &M, const uint32_t *bin,
+                                                 const bb *set, bb occ, uint64_t idx,
+                                                 DevStatus *st) {
+  const DIdx &X = M.ii;
+  const bb kings = bit(J.k0) | bit(J.k1);
+  const int opp = J.stm ? J.k0 : J.k1;
+  const int me = J.stm ? J.k1 : J.k0;
+  const bb dest = ~(occ | king_attacks(opp));
+  for (int d = 0; d < J.nk; d++) {
+    const KingDest &D = kd[d];
+    if (!(dest & bit(D.to))) continue;
+    const uint64_t i =
+        (D.mirror == 0 && D.flip == 0)
+            ? idx + cross_delta<NS>(X, bin, set, kings, 0, me, D.to)
+            : rank_mod<NS>(X, bin, D.k0, D.k1, set, -1, 0, -1, 0, D.mirror, D.flip);
+    mark(D.bits, i, X.size, st);
+    if (D.dbl) {
+      // mirror_diagonal (tb8gen.c:240-244) of the normalised position
+      const uint64_t i2 = rank_mod<NS>(X, bin, D.k0, D.k1, set, -1, 0, -1, 0, D.mirror, D.flip ^ 1);
+      mark(D.bits, i2, X.size, st);
+    }
+  }
+  bb occk = kings;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    if (M.set_color[k] == J.stm) {
+      const bool inc = X.mult[k] <= 4;
+      const uint64_t base = idx - (uint64_t)rank_one(set[k], occk, bin) * X.factor[k];
+      const int type = M.set_type[k];
+      bb pcs = set[k];
+      while (pcs) {
+        const int x = pop_lsb(pcs);
+        Mover mv;
+        if (inc) mover_init(mv, bin, set[k], x, occk);
+        auto index_of = [&](int to) -> uint64_t {
+          return inc ? base + (uint64_t)mover_rank(mv, bin, to, occk) * X.factor[k] +
+                           cross_delta<NS>(X, bin, set, kings, k + 1, x, to)
+                     : rank_mod<NS>(X, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0);
+        };
+        if (J.filter != nullptr && type >= 3 && type <= 5) {
+          const int d0 = type == 3 ? 4 : 0, d1 = type == 4 ? 4 : 8;
+          for (int d = d0; d < d1; d++) {
+            // directions: 0 E, 1 W, 2 N, 3 S, 4 NE, 5 NW, 6 SE, 7 SW
+            const int df = (d == 0 || d == 4 || d == 6) ? 1 : (d == 1 || d == 5 || d == 7) ? -1 : 0;
+            const int dr = (d == 2 || d == 4 || d == 5) ? 1 : (d == 3 || d == 6 || d == 7) ? -1 : 0;
+            int f = x & 7, r = x >> 3, n = 0;
+            uint64_t i_prev = 0, i_first = 0;
+            for (;;) {
+              f += df;
+              r += dr;
+              if ((unsigned)f > 7u || (unsigned)r > 7u) break;
+              const int to = r * 8 + f;
+              if ((occ >> to) & 1) break;
+              const uint64_t i = index_of(to);
+              if (n == 0) {
+                i_first = i;
+              } else {
+                if (n == 1 && test(J.filter, i, X.size, st)) mark(J.self, i_first, X.size, st);
+                if (test(J.filter, i_prev, X.size, st)) mark(J.self, i, X.size, st);
+              }
+              i_prev = i;
+              n++;
+            }
+            if (n == 1) mark(J.self, i_first, X.size, st);
+          }
+        } else {
+          bb to_set = piece_attacks(type, x, occ) & ~occ;
+          while (to_set) mark(J.self, index_of(pop_lsb(to_set)), X.size, st);
+        }
+      }
+    }
+    occk |= set[k];
+  }
+}
+
+// The sources of tiles [t0, t0 + ntile) of bits[] (within each tile only
+// its words [lo, hi)), gathered into one shared list until it holds
+// kFlush entries (or a tile's sources do not fit), then handed to f(idx)
+// in contiguous shares: every thread of the block gets the same number of
+// sources, give or take one, and neighbouring indices.  An entry is the
+// tile's place in the group (bits 15 and up) and the position's offset in
+// its tile.
+constexpr int kFlush = 1024;
+
+template <class F>
+__device__ __forceinline__ void scan_group(uint64_t t0, int ntile, const uint32_t *bits,
+                                           uint64_t nbits, uint32_t *list, int *list_n, F &&f,
+                                           int lo = 0, int hi = kTileWords) {
+  const uint64_t nwords = (nbits + 31) >> 5;
+  const int lane = threadIdx.x & 31;
+  const bool mine = threadIdx.x * 4 >= lo && threadIdx.x * 4 < hi;
+  if (threadIdx.x == 0) *list_n = 0;
+  __syncthreads();
+  for (int g = 0; g < ntile; g++) {
+    const uint64_t t = t0 + g;
+    const uint64_t w0 = t * kTileWords + threadIdx.x * 4;
+    uint32_t w[4];
+    if (w0 + 4 <= nwords) {
+      const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(bits + w0));
+      w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; i++) w[i] = w0 + i < nwords ? bits[w0 + i] : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const uint64_t base = (w0 + i) * 32;
+      if (base + 32 > nbits) w[i] &= base < nbits ? (1u << (nbits - base)) - 1u : 0u;
+      if (!mine) w[i] = 0;
+    }
+    for (;;) {
+      const int c = __popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]);
+      int incl = c;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += y;
+      }
+      int base = 0;
+      if (lane == 31 && incl) base = atomicAdd(list_n, incl);
+      base = __shfl_sync(0xffffffffu, base, 31);
+      int pos = base + incl - c;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        while (w[i] && pos < kListCap) {
+          const int b = __ffs(w[i]) - 1;
+          w[i] &= w[i] - 1;
+          list[pos++] = ((uint32_t)g << 15) | (uint32_t)((threadIdx.x * 4 + i) * 32 + b);
+        }
+      }
+      const int more = __syncthreads_or((w[0] | w[1] | w[2] | w[3]) != 0);
+      const int n = min(*list_n, kListCap);
+      // every thread has read the count before the next tile appends
+      __syncthreads();
+      if (more || n >= kFlush || g == ntile - 1) {
+        int e0, e1;
+        my_share(n, e0, e1);
+        for (int e = e0; e < e1; e++) {
+          const uint32_t v = list[e];
+          f((t0 + (v >> 15)) * (uint64_t)(kTileWords * 32) + (v & 32767u));
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) *list_n = 0;
+        __syncthreads();
+      }
+      if (!more) break;
+    }
+  }
+}
+
 // Shared memory of the sparse kernels (one tile at a time).
 struct SparseSmem {
   uint32_t bin[7 * 64];
@@ -589,25 +848,22 @@ struct SparseSmem {
   int n2[2];
 };
 
-// One tile of predecessors_worker (tb8gen.c:484-516).
+// Tiles [t0, t0 + ntile) of predecessors_worker (tb8gen.c:484-516): every
+// source's unmoves marked (within each tile only the words [lo, hi)).
 template <int NS>
-__device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem &S, uint64_t t,
-                                                  DevStatus *st, int lo = 0,
+__device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem &S, uint64_t t0,
+                                                  int ntile, DevStatus *st, int lo = 0,
                                                   int hi = kTileWords) {
   const DMat &M = c_mats[J.mat];
   bb set[NS];
   RowCache rc;
-  scan_tile<false, true>(
-      t, const_cast<uint32_t *>(J.src), J.nbits, S.list, nullptr, &S.list_n,
+  scan_group(
+      t0, ntile, J.src, J.nbits, S.list, &S.list_n,
       [&](uint64_t idx) {
-        bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
-        RankCtx<NS> c;
-        rank_ctx<NS>(c, M.ii, S.bin, J.k0, J.k1, set);
-        mark_king_unmoves<NS>(J, S.kd, M, S.bin, set, occ, -1, 0, st, &c);
-        mark_piece_unmoves<NS>(J, M, S.bin, set, occ, -1, st, &c);
-        return false;
+        const bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
+        mark_unmoves_inc<NS>(J, S.kd, M, S.bin, set, occ, idx, st);
       },
-      nullptr, NoHook(), NoHook(), lo, hi);
+      lo, hi);
 }
 
 // A tile of a small bitmap is cut into `nsplit` parts of consecutive words
@@ -620,19 +876,30 @@ __device__ __forceinline__ void part_of(uint64_t u, int nsplit, uint64_t &t, int
   hi = lo + kTileWords / nsplit;
 }
 
+// Work units: with nsplit > 1 (a bitmap of few tiles) a part of a tile;
+// otherwise a group of gt consecutive tiles.
 template <int NS>
-__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors(SliceJob J, DevStatus *st,
-                                                                            int nsplit) {
+__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER)
+k_predecessors(SliceJob J, DevStatus *st, int nsplit, int gt) {
   __shared__ SparseSmem S;
   load_dests(J, S.kd);
   load_binomials(S.bin);
   __syncthreads();
-  const uint64_t nu = tiles_of(J.nbits) * (uint64_t)nsplit;
+  const uint64_t tiles = tiles_of(J.nbits);
+  if (nsplit > 1) {
+    const uint64_t nu = tiles * (uint64_t)nsplit;
+    for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
+      uint64_t t;
+      int lo, hi;
+      part_of(u, nsplit, t, lo, hi);
+      tile_predecessors<NS>(J, S, t, 1, st, lo, hi);
+    }
+    return;
+  }
+  const uint64_t nu = (tiles + gt - 1) / gt;
   for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
-    uint64_t t;
-    int lo, hi;
-    part_of(u, nsplit, t, lo, hi);
-    tile_predecessors<NS>(J, S, t, st, lo, hi);
+    const uint64_t t0 = u * gt;
+    tile_predecessors<NS>(J, S, t0, (int)min((uint64_t)gt, tiles - t0), st);
   }
 }
 

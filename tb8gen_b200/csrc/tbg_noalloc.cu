@@ -21,6 +21,7 @@
 // every partial it later reads, so nothing needs clearing between calls.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "../../include/tbgpu.h"
@@ -34,8 +35,11 @@ constexpr int kEpiThreads = 256;
 // partials[0 .. kMaxChunks-1], total at [kMaxChunks].
 static __device__ __align__(256) unsigned long long g_epi_scratch[kMaxChunks + 1];
 
+// Device address of the scratch array per device ordinal, looked up once.
+// It stays valid for the life of the device's primary context: a process
+// that calls cudaDeviceReset must not use this entry point afterwards.
 constexpr int kMaxDevices = 64;
-static void *g_scratch_addr[kMaxDevices];
+static std::atomic<void *> g_scratch_addr[kMaxDevices];
 
 // Block b owns bytes [b * kChunkBytes, min((b + 1) * kChunkBytes, bytes)):
 // T &= ~wins_in, wins_out = wins_in | T, partial[b] = popcount of T below
@@ -92,12 +96,12 @@ int scratch_address(unsigned long long **out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return TBG_ERR_CUDA;
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
+  void *p = g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!p) {
     if (cudaGetSymbolAddress(&p, g_epi_scratch) != cudaSuccess || !p) return TBG_ERR_CUDA;
-    g_scratch_addr[dev] = p;
+    g_scratch_addr[dev].store(p, std::memory_order_release);
   }
-  *out = static_cast<unsigned long long *>(g_scratch_addr[dev]);
+  *out = static_cast<unsigned long long *>(p);
   return TBG_OK;
 }
 
@@ -117,11 +121,21 @@ extern "C" int tbg_epilogue_W_static(void *dev_T, const void *dev_wins_in, void 
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int nchunks = (int)((bytes + kChunkBytes - 1) / kChunkBytes);
-  k_epilogue_static<<<nchunks, kEpiThreads, 0, st>>>(
-      static_cast<uint4 *>(dev_T), static_cast<const uint4 *>(dev_wins_in),
-      static_cast<uint4 *>(dev_wins_out), bytes, nbits, scratch);
-  k_epilogue_static_total<<<1, 1024, 0, st>>>(scratch, nchunks);
-  if (cudaGetLastError() != cudaSuccess) return TBG_ERR_CUDA;
+  // Launched through cudaLaunchKernel, whose status is this launch's own
+  // (cudaGetLastError would also return an error left by an earlier,
+  // unrelated call of the caller's).
+  uint4 *T = static_cast<uint4 *>(dev_T);
+  const uint4 *win = static_cast<const uint4 *>(dev_wins_in);
+  uint4 *wout = static_cast<uint4 *>(dev_wins_out);
+  void *a1[] = {&T, &win, &wout, &bytes, &nbits, &scratch};
+  if (cudaLaunchKernel((const void *)k_epilogue_static, dim3(nchunks), dim3(kEpiThreads), a1, 0,
+                       st) != cudaSuccess)
+    return TBG_ERR_CUDA;
+  int nch = nchunks;
+  void *a2[] = {&scratch, &nch};
+  if (cudaLaunchKernel((const void *)k_epilogue_static_total, dim3(1), dim3(1024), a2, 0, st) !=
+      cudaSuccess)
+    return TBG_ERR_CUDA;
   unsigned long long total = 0;
   if (cudaMemcpyAsync(&total, scratch + kMaxChunks, sizeof total, cudaMemcpyDeviceToHost, st) !=
       cudaSuccess)

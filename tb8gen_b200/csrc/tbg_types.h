@@ -64,6 +64,8 @@ struct SliceJob {
   uint32_t *self;         // bitmap bound to slice s
   const uint8_t *self_sub;
   uint64_t self_sub_len;
+  const uint32_t *filter; // candidates: the opponent's "wins" of slice s (or null)
+  uint64_t pad;
   KingDest kd[8];
 };
 
@@ -92,6 +94,8 @@ struct alignas(16) Op {
   uint32_t ntiles;
   int npred, pred_off;
   int cnt_slot;            // epilogue count slot of a recorded batch (-1: none)
+  int gt;                  // scatter: tiles per work item (1: one tile)
+  int pad;
   uint64_t first;          // index of the op's first work item
   SliceJob J;              // sparse kernels
   uint32_t *out;           // verify: out-of-place output (or null)

@@ -243,8 +243,10 @@ static int calc_L_n(int stm, int n, int more_l)
       ok(tbg_predecessors_sub(stm, s, 0), "predecessors_sub");
     }
     if (more_l && n > 1) {
+      /* predecessors() less those a slider step takes out of stm^1's wins,
+       * which the verify below would clear (tbg_candidates) */
       ok(tbg_slot_bind(-1, Wp[stm ^ 1][s], g_bytes), "bind");
-      ok(tbg_predecessors(stm, s), "predecessors");
+      ok(tbg_candidates(stm, s, wins[stm ^ 1][s], g_bytes), "candidates");
     }
   }
   /* verify against stm^1's wins and winning captures */
@@ -881,7 +883,10 @@ static void compute(const Part *P, int h, int64_t q)
       }
       if (has_src(P, s)) {
         ok(tbg_slot_bind(-1, st_src[p][j], g_bytes), "bind");
-        ok(tbg_predecessors(stm, s), "predecessors");
+        if (P->kind == PART_CAND && g_dwins[stm ^ 1])
+          ok(tbg_candidates(stm, s, DWIN(stm ^ 1, s), g_bytes), "candidates");
+        else
+          ok(tbg_predecessors(stm, s), "predecessors");
       }
     }
     if (P->kind == PART_W)

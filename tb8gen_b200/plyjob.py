@@ -8,10 +8,13 @@ For slice s, white to move in the W step (black in the L step):
           (marks into s and its white-king slices, tb8gen.c:1051-1054);
           epilogue: W(s) = T(s) & ~wins_in, wins_out = wins_in | W(s)
           (tb8gen.c:1072-1077).
-  L step  clear X(s); predecessors(BLACK, s) from W_prev = W^w_{n-1}(s)
-          (candidates, tb8gen.c:972-975); check_successors(BLACK, s) against
-          white's "wins" of s and its black-king slices and white's sub/win
-          (tb8gen.c:1000-1017); X(s) then holds L(s).
+  L step  clear X(s); candidates(BLACK, s) from W_prev = W^w_{n-1}(s)
+          (predecessors() of tb8gen.c:972-975, less the predecessors a
+          slider step takes out of white's wins(s), which the verify would
+          clear; filtered=False: predecessors() itself);
+          check_successors(BLACK, s) against white's "wins" of s and its
+          black-king slices and white's sub/win (tb8gen.c:1000-1017); X(s)
+          then holds L(s).
 
 Inputs are seeded: L_prev and W_prev are Bernoulli(p) bitmaps with the
 positions illegal for their side to move cleared, wins_in(s) and the
@@ -157,8 +160,9 @@ class SlicePly:
     """Buffers and step of one slice-ply job (see module docstring)."""
 
     def __init__(self, material: str, s: int, p: float, seed: int,
-                 pool: MaterialPool | None = None):
+                 pool: MaterialPool | None = None, filtered: bool = True):
         self.material, self.s, self.p, self.seed = material, s, p, seed
+        self.filtered = filtered
         self.pool = pool
         self.m = pool.m if pool is not None else tbg.Material(material)
         self.m.select()
@@ -232,7 +236,12 @@ class SlicePly:
         for t, buf in self.X_nbr.items():
             tbg.bind(t, buf)
         tbg.clear(self.s)
-        tbg.predecessors(BLACK, self.s)
+        if self.filtered:
+            # candidates that a slider step leaves in white's wins(s) only:
+            # l_verify clears the others anyway
+            tbg.candidates(BLACK, self.s, self.wins)
+        else:
+            tbg.predecessors(BLACK, self.s)
 
     def l_verify(self):
         self.m.select()
