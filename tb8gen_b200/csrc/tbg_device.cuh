@@ -30,7 +30,7 @@ __device__ __forceinline__ int msb64(bb b) { return 63 - __clzll((long long)b); 
 // quintessence", chessprogramming wiki): for a line mask m that excludes the
 // origin s, attacks = ((o - 2s) ^ rev(rev(o) - 2 rev(s))) & m with o = occ & m.
 // No lookup table; the reference's magic tables (magic.h:23-38) are matched
-// exhaustively in tests/test_gpu_tables.py.
+// exhaustively in tests/test_gpu_parity.py::test_attacks_exhaustive.
 __device__ __forceinline__ bb line_attacks(bb occ, int sq, bb mask) {
   bb o = occ & mask;
   bb s = bit(sq);
