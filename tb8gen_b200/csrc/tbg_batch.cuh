@@ -9,7 +9,9 @@
 // write-after-write; two scatters into one bitmap commute and do not
 // conflict; the waits of the listed ops cover older accesses).  A CTA takes the next item with one atomicAdd, waits -- with an
 // iteration bound -- until the item's predecessor ops have all their tiles
-// done, runs the tile and counts it done.  Items are taken in record order,
+// done, runs the tile and counts it done (at its next fetch, after the
+// block's barrier).  Consecutive items of one op reuse the op's descriptor
+// in shared memory.  Items are taken in record order,
 // so every predecessor of the earliest unfinished item was taken earlier and
 // is finished: that item can always proceed, whatever the grid size.
 #pragma once
@@ -90,9 +92,16 @@ k_batch(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, uin
   __shared__ unsigned long long s_item;
   __shared__ int s_op, s_abort;
   load_binomials(S.bin);
+  int cur_op = -1;   // the op whose descriptor (and king destinations) are in `so`
+  int prev_op = -1;  // thread 0: the op of the item this block finished last
   for (;;) {
+    // every thread has finished the previous item (and read `so` and S.kd)
     __syncthreads();
     if (threadIdx.x == 0) {
+      if (prev_op >= 0) {
+        __threadfence();
+        atomicAdd(&done[prev_op], 1u);
+      }
       unsigned long long it = atomicAdd(next, 1ull);
       s_item = it;
       s_abort = 0;
@@ -123,18 +132,23 @@ k_batch(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, uin
     __syncthreads();
     if (s_item >= total || s_abort) break;
     __threadfence();
-    {  // the op's descriptor into shared memory
-      const int4 *src = reinterpret_cast<const int4 *>(&ops[s_op]);
+    const int op = s_op;
+    if (op != cur_op) {
+      // a new op: its descriptor (and its king destinations) into shared memory
+      const int4 *src = reinterpret_cast<const int4 *>(&ops[op]);
       int4 *dst = reinterpret_cast<int4 *>(&so);
       for (int i = threadIdx.x; i < (int)(sizeof(Op) / 16); i += blockDim.x) dst[i] = src[i];
+      __syncthreads();
+      if (!op_streams(so.kind)) {
+        load_dests(so.J, S.kd);
+        __syncthreads();
+      }
+      cur_op = op;
     }
-    __syncthreads();
     const uint64_t t = s_item - so.first;
     if (op_streams(so.kind)) {
       tile_stream(so, t);
     } else {
-      load_dests(so.J, S.kd);
-      __syncthreads();
       switch (so.ns) {
       case 1: tile_sparse<1>(so, S, t, st); break;
       case 2: if (NSMAX >= 2) tile_sparse<(NSMAX >= 2 ? 2 : 1)>(so, S, t, st); break;
@@ -144,11 +158,8 @@ k_batch(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, uin
       default: if (NSMAX >= 6) tile_sparse<(NSMAX >= 6 ? 6 : 1)>(so, S, t, st); break;
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      atomicAdd(&done[s_op], 1u);
-    }
+    // counted done at the top of the next iteration, after its barrier
+    prev_op = op;
   }
 }
 
