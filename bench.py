@@ -325,7 +325,7 @@ def run_engine(a, rank, world, local):
     mix = None
     if a.workload == "slice" and not a.no_mix:
         mix = mix_record(a, stream)
-        tbg.batch_shape(best_gt)  # the timed batch's shape for what follows
+        tbg.batch_shape(*best_gt)  # the timed batch's shape for what follows
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -374,7 +374,8 @@ def run_engine(a, rank, world, local):
         "paths_ms": {"plain": round(plain_ms, 4), "batched": round(batched_ms, 4),
                      "batched_speedup": round(plain_ms / batched_ms, 3)},
         "batch": {"calls": nops, "work_items": nitems, "ctas_per_sm": best_cps,
-                  "scatter_tiles": best_gt, "autotune_ms": tune},
+                  "tiles_per_item": {"predecessors": best_gt[0], "candidates": best_gt[1]},
+                  "autotune_ms": tune},
         "counts_first_jobs": counts,
         "roofline": roofline, "gpu_launches": launches, "clocks": clk,
         "e2e": e2e, "cpu_baseline": cpu,
@@ -400,26 +401,29 @@ def time_batch(tbg, stream, md, reps):
     return e0.elapsed_time(e1) / reps
 
 
-TUNE_CPS = (2, 3, 4)
-TUNE_SCATTER_TILES = (1, 2, 4)
+TUNE_CPS = (3, 4)
+TUNE_SCATTER_TILES = (1, 2)
+TUNE_CANDIDATE_TILES = (1, 2, 4, 8)
 
 
 def autotune(tbg, time_mode, fixed_cps=0):
     """The persistent launch's shape picked on the recorded batch by its own
     device time: CTAs per SM (the blocks that take work items at once) x
-    tiles per scatter work item (the sources a block gathers before handing
-    them out).  Returns ({"<cps>x<tiles>": ms}, cps, tiles, work items)."""
+    tiles per work item of the W step's scatter x tiles per work item of
+    the L step's candidates (the sources a block gathers before handing
+    them out).  Returns ({"<cps>x<w>x<l>": ms}, cps, (w, l), work items)."""
     tune = {}
-    for gt in TUNE_SCATTER_TILES:
-        tbg.batch_shape(gt)
-        for cps in ((fixed_cps,) if fixed_cps > 0 else TUNE_CPS):
-            tbg.batch_tune(cps)
-            tune[f"{cps}x{gt}"] = round(time_mode(1, 2), 4)
+    for gw in TUNE_SCATTER_TILES:
+        for gl in TUNE_CANDIDATE_TILES:
+            tbg.batch_shape(gw, gl)
+            for cps in ((fixed_cps,) if fixed_cps > 0 else TUNE_CPS):
+                tbg.batch_tune(cps)
+                tune[f"{cps}x{gw}x{gl}"] = round(time_mode(1, 2), 4)
     best = min(tune, key=tune.get)
-    cps, gt = (int(x) for x in best.split("x"))
-    nitems = tbg.batch_shape(gt)
+    cps, gw, gl = (int(x) for x in best.split("x"))
+    nitems = tbg.batch_shape(gw, gl)
     tbg.batch_tune(cps)
-    return tune, cps, gt, nitems
+    return tune, cps, (gw, gl), nitems
 
 
 def mix_record(a, stream, slot=2):
@@ -470,7 +474,8 @@ def mix_record(a, stream, slot=2):
            "materials": sorted(pools), "plain_ms": round(plain, 3),
            "batched_ms": round(batched, 3), "batched_speedup": round(plain / batched, 3),
            "value_batched": round(positions / (batched / 1e3), 1),
-           "calls": nops, "work_items": nitems, "ctas_per_sm": cps, "scatter_tiles": gt,
+           "calls": nops, "work_items": nitems, "ctas_per_sm": cps,
+           "tiles_per_item": {"predecessors": gt[0], "candidates": gt[1]},
            "autotune_ms": tune,
            "parity": {"golden": ("differ" if bad else "equal") if checked else "not recorded",
                       "slices_checked": checked, "mismatches": bad}}

@@ -291,14 +291,16 @@ int tbg_batch_counts_async(uint64_t *host_out, int n);
  * a batch is being recorded. */
 int tbg_batch_select(int slot);
 
-/* Work-item shape of scatters (tiles of 32,768 positions per item of the
- * persistent queue and per block of a plain launch; 0: one tile): a block
- * gathers the sources of an item's tiles before handing them out to its
- * threads.  Applies to later recordings and re-cuts the selected recorded
- * batch (*nitems: its work items now, 0 if none is recorded; nitems may be
- * NULL).  Results do not depend on it.  No counterpart in the reference
- * (its g_total_work ranges, tb8gen.c:1327, are the nearest knob). */
-int tbg_batch_shape(int scatter_tiles, uint64_t *nitems);
+/* Work-item shape of the scatters, in tiles of 32,768 positions per item of
+ * the persistent queue and per block of a plain launch: scatter_tiles for
+ * tbg_predecessors (0: 1), candidate_tiles for tbg_candidates (0: 4).  A
+ * block gathers the sources of an item's tiles before handing them out to
+ * its threads.  Applies to later recordings and re-cuts the selected
+ * recorded batch (*nitems: its work items now, 0 if none is recorded;
+ * nitems may be NULL).  Results do not depend on it.  No counterpart in the
+ * reference (its g_total_work ranges, tb8gen.c:1327, are the nearest
+ * knob). */
+int tbg_batch_shape(int scatter_tiles, int candidate_tiles, uint64_t *nitems);
 
 /* Persistent-launch configuration of every slot: CTAs per SM (default 4),
  * and the iteration bound of a dependency wait (<= 0 keeps the current

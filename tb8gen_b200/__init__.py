@@ -75,7 +75,7 @@ def lib():
             "tbg_batch_run": [i],
             "tbg_batch_counts": [C.POINTER(u64), i],
             "tbg_batch_tune": [i, C.c_longlong],
-            "tbg_batch_shape": [i, C.POINTER(u64)],
+            "tbg_batch_shape": [i, i, C.POINTER(u64)],
             "tbg_batch_select": [i],
             "tbg_batch_count": [i],
             "tbg_mark": [C.POINTER(u64)],
@@ -301,11 +301,12 @@ def batch_tune(ctas_per_sm: int, spin_limit: int = 0):
     check(lib().tbg_batch_tune(ctas_per_sm, spin_limit))
 
 
-def batch_shape(scatter_tiles: int = 0) -> int:
-    """Tiles per scatter work item (0: one); re-cuts the selected recorded
-    batch and returns its work items (0 if none is recorded)."""
+def batch_shape(scatter_tiles: int = 0, candidate_tiles: int = 0) -> int:
+    """Tiles per work item of predecessors (0: 1) and of candidates (0: 4);
+    re-cuts the selected recorded batch and returns its work items (0 if
+    none is recorded)."""
     n = C.c_uint64()
-    check(lib().tbg_batch_shape(scatter_tiles, C.byref(n)))
+    check(lib().tbg_batch_shape(scatter_tiles, candidate_tiles, C.byref(n)))
     return n.value
 
 

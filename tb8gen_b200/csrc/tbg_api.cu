@@ -506,15 +506,21 @@ extern "C" int tbg_unbind_all(void) {
 // Every call of the ply step becomes an Op; outside a recording it is
 // launched at once, inside one it is appended to the batch.
 // Work items of an op: 1 MiB chunks of a streaming op, tiles of a verify
-// or an uncapture, groups of gt tiles of a scatter (tbg_batch_shape; one
-// tile unless set): a scatter's block gathers the sparse sources of an
-// item's tiles before handing them out.
+// or an uncapture, groups of gt tiles of a scatter (tbg_batch_shape; by
+// default one tile for predecessors, four for candidates): a scatter's
+// block gathers the sparse sources of an item's tiles before handing them
+// out.
 static uint32_t op_tiles(Op &o) {
   o.gt = 1;
   if (op_streams(o.kind)) return (uint32_t)((o.n16 + kChunk16 - 1) / kChunk16);
   const uint64_t tiles = (o.J.nbits + kTileWords * 32ull - 1) / (kTileWords * 32ull);
   if (o.kind == OP_SCATTER) {
-    const uint64_t g = g_eng.scatter_tiles > 0 ? (uint64_t)g_eng.scatter_tiles : 1;
+    // candidates (tbg_candidates) mark only near their source's row and read
+    // the opponent's wins there: larger items pay; a plain scatter's marks
+    // spread over the slice, and the fewer tiles in flight the better its
+    // targets stay in L2
+    const int want = o.J.filter ? g_eng.candidate_tiles : g_eng.scatter_tiles;
+    const uint64_t g = want > 0 ? (uint64_t)want : (o.J.filter ? 4 : 1);
     o.gt = (int)std::min<uint64_t>(std::max<uint64_t>(g, 1), std::max<uint64_t>(tiles, 1));
   }
   return (uint32_t)((tiles + o.gt - 1) / o.gt);
@@ -1066,11 +1072,13 @@ extern "C" int tbg_batch_select(int slot) {
   return TBG_OK;
 }
 
-extern "C" int tbg_batch_shape(int scatter_tiles, uint64_t *nitems) {
-  if (scatter_tiles < 0 || scatter_tiles > 64) return fail(TBG_ERR_ARG, "scatter_tiles 0..64");
+extern "C" int tbg_batch_shape(int scatter_tiles, int candidate_tiles, uint64_t *nitems) {
+  if (scatter_tiles < 0 || scatter_tiles > 64 || candidate_tiles < 0 || candidate_tiles > 64)
+    return fail(TBG_ERR_ARG, "tiles per item 0..64");
   for (const Batch &b : g_eng.batches)
     if (b.recording) return fail(TBG_ERR_STATE, "a batch is being recorded");
   g_eng.scatter_tiles = scatter_tiles;
+  g_eng.candidate_tiles = candidate_tiles;
   Batch &b = g_eng.batch();
   if (nitems) *nitems = 0;
   if (!b.ready) return TBG_OK;

@@ -94,7 +94,8 @@ struct Engine {
   int bps_scatter = 8;    // grid = SMs x this for the sparse kernels (tiles loop)
   int bps_verify = 8;
   int max_split = 64;     // parts per tile for small bitmaps (tbg_tune_split)
-  int scatter_tiles = 0;  // tiles per scatter work item (tbg_batch_shape; 0: one)
+  int scatter_tiles = 0;    // tiles per predecessors work item (tbg_batch_shape; 0: 1)
+  int candidate_tiles = 0;  // tiles per candidates work item (0: 4)
   // Recorded batches: kBatchSlots slots, one selected (tbg_batch_select).
   static constexpr int kBatchSlots = 4;
   Batch batches[kBatchSlots];

@@ -272,9 +272,14 @@ __device__ __forceinline__ int compact_round(uint32_t *w, uint32_t *list, int *l
 }
 
 // This thread's contiguous share [e0, e1) of n list entries.
+// The n % blockDim.x threads that take one entry more are the lowest ones,
+// so they fill whole warps: a warp runs as long as its busiest lane, and
+// spreading the extra entries over every warp would make every warp run
+// the longer time.
 __device__ __forceinline__ void my_share(int n, int &e0, int &e1) {
-  e0 = (int)(((long)n * threadIdx.x) / blockDim.x);
-  e1 = (int)(((long)n * (threadIdx.x + 1)) / blockDim.x);
+  const int q = n / (int)blockDim.x, r = n % (int)blockDim.x, t = threadIdx.x;
+  e0 = t * q + min(t, r);
+  e1 = e0 + q + (t < r ? 1 : 0);
 }
 
 // The verify's scan of one tile in two passes per compaction round: quick(idx)
@@ -415,8 +420,7 @@ __device__ __forceinline__ void scan_tile(uint64_t t, uint32_t *bits, uint64_t n
     const uint64_t tbase = t * (uint64_t)kTileWords * 32;
     int e0, e1, es;
     if (kContig) {
-      e0 = (int)(((long)n * threadIdx.x) / blockDim.x);
-      e1 = (int)(((long)n * (threadIdx.x + 1)) / blockDim.x);
+      my_share(n, e0, e1);
       es = 1;
     } else {
       e0 = threadIdx.x;

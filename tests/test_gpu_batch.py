@@ -171,3 +171,24 @@ def test_batch_slots(setup):
             for n, t in zip(names, bufs):
                 setattr(j, n, t)
         tbg.unbind_all()
+
+
+def test_item_shapes_do_not_change_results(setup):
+    """Tiles per work item of the scatters and of the filtered candidates
+    (tbg_batch_shape) re-cut the recorded batch; every shape, persistent and
+    plain, gives the same bitmaps."""
+    torch, tbg, jobs, pools, nops = setup
+    try:
+        tbg.batch_shape(1, 1)
+        (a, sa), ca = run(torch, tbg, jobs, pools, 1, 4)
+        for gw, gl in ((2, 4), (4, 8), (1, 16)):
+            n = tbg.batch_shape(gw, gl)
+            assert n > 0
+            for mode in (1, 0):
+                (b, sb), cb = run(torch, tbg, jobs, pools, mode, 3)
+                assert ca == cb
+                for x, y in zip(a, b):
+                    for u, v in zip(x, y):
+                        assert np.array_equal(u, v)
+    finally:
+        tbg.batch_shape(0, 0)
