@@ -79,6 +79,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mix", action="store_true",
                     help="slice workload: skip the uneven-mix record (batched vs plain)")
+    ap.add_argument("--no-probe", action="store_true",
+                    help="slice workload: skip the probe record (config 3)")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="slice workload: skip the serving record (config 4)")
     return ap.parse_args()
 
 
@@ -362,6 +366,16 @@ def run_engine(a, rank, world, local):
     parity = slice_parity(jobs, ref_ply)
     del ref_ply
 
+    # configs 3 and 4 beside the timed workload, each its own full record
+    probe = serve = None
+    if a.workload == "slice" and world == 1:
+        if not a.no_probe:
+            probe = embedded(run_probe(a, rank, world, local))
+            torch.cuda.empty_cache()
+        if not a.no_serve:
+            serve = embedded(run_serve(a, rank, world, local))
+            torch.cuda.empty_cache()
+
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 4),
@@ -379,9 +393,17 @@ def run_engine(a, rank, world, local):
         "counts_first_jobs": counts,
         "roofline": roofline, "gpu_launches": launches, "clocks": clk,
         "e2e": e2e, "cpu_baseline": cpu,
-        "mix": mix,
+        "mix": mix, "probe": probe, "serve": serve,
     }
     return line
+
+
+def embedded(line):
+    """A workload's own bench line, as a record inside the default line."""
+    if line is None:
+        return None
+    drop = ("n_gpus", "higher_is_better", "scaling", "vs_baseline", "data", "gpu_launches")
+    return {k: v for k, v in line.items() if k not in drop}
 
 
 def time_batch(tbg, stream, md, reps):
@@ -1439,7 +1461,10 @@ def main():
             print(json.dumps(line), flush=True)
             par = line.get("parity") or {}
             mixpar = ((line.get("mix") or {}).get("parity") or {}).get("golden")
-            if "differ" in (par.get("golden"), par.get("vs_reference"), mixpar):
+            probe_ok = ((line.get("probe") or {}).get("cpu_baseline") or {}).get(
+                "sample_bit_exact", True)
+            if "differ" in (par.get("golden"), par.get("vs_reference"), mixpar) or \
+                    probe_ok is False:
                 sys.stderr.write("bench: outputs differ from the reference: "
                                  f"{par.get('mismatches')}\n")
                 sys.exit(1)
