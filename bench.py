@@ -423,7 +423,7 @@ def time_batch(tbg, stream, md, reps):
     return e0.elapsed_time(e1) / reps
 
 
-TUNE_CPS = (3, 4)
+TUNE_CPS = (3, 4, 6, 8)
 TUNE_SCATTER_TILES = (1, 2)
 TUNE_CANDIDATE_TILES = (1, 2, 4, 8)
 

@@ -891,7 +891,7 @@ extern "C" int tbg_attacks(int type, const uint8_t *dev_sq, const uint64_t *dev_
                            uint64_t *dev_out, uint64_t n) {
   if (!g_eng.dev_ready) return fail(TBG_ERR_STATE, "tbg_init not called");
   if (type < 2 || type > 6 || !dev_sq || !dev_occ || !dev_out) return fail(TBG_ERR_ARG, "bad args");
-  k_attacks<<<g_eng.grid_for((n + 255) / 256, 8), 256, 0, g_eng.stream>>>(type, dev_sq, dev_occ,
+  k_attacks<<<g_eng.grid_for((n + kThreads - 1) / kThreads, 8), kThreads, 0, g_eng.stream>>>(type, dev_sq, dev_occ,
                                                                         dev_out, n);
   return g_eng.check_launch("k_attacks");
 }

@@ -21,7 +21,7 @@
 namespace tbg {
 
 #ifndef TBG_MINB_BATCH
-#define TBG_MINB_BATCH 4
+#define TBG_MINB_BATCH (1024 / TBG_THREADS)
 #endif
 
 __device__ __forceinline__ unsigned int load_acquire(const unsigned int *p) {

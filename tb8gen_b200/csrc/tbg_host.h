@@ -1,6 +1,10 @@
 // Host-side state of the engine: king-slice tables, materials, slot map.
 #pragma once
 
+#ifndef TBG_THREADS
+#define TBG_THREADS 256
+#endif
+
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -71,7 +75,7 @@ struct Batch {
   size_t cap_counts = 0;
   unsigned long long *d_next = nullptr;
   // persistent launch configuration
-  int ctas_per_sm = 4;
+  int ctas_per_sm = 1024 / TBG_THREADS;
   long long spin_limit = 50000000;
 
   void clear();

@@ -20,17 +20,22 @@
 
 namespace tbg {
 
-// Blocks per SM the sparse kernels are compiled for (register budget).
+// Threads per block of every kernel (a sparse tile is 4 words per thread)
+// and blocks per SM the sparse kernels are compiled for: 1,024 resident
+// threads at 64 registers each.
+#ifndef TBG_THREADS
+#define TBG_THREADS 256
+#endif
 #ifndef TBG_MINB_VERIFY
-#define TBG_MINB_VERIFY 4
+#define TBG_MINB_VERIFY (1024 / TBG_THREADS)
 #endif
 #ifndef TBG_MINB_SCATTER
-#define TBG_MINB_SCATTER 4
+#define TBG_MINB_SCATTER (1024 / TBG_THREADS)
 #endif
 
-constexpr int kThreads = 256;
-constexpr int kTileWords = kThreads * 4;      // 1024 words = 32768 positions
-constexpr int kListCap = 4096;
+constexpr int kThreads = TBG_THREADS;
+constexpr int kTileWords = kThreads * 4;      // 1024 words = 32768 positions at 256
+constexpr int kListCap = kThreads * 16;
 
 // Materials and stub parameters, uniform across a launch: constant memory.
 // (This header is compiled into exactly one translation unit, tbg_api.cu.)
@@ -773,7 +778,7 @@ __device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDe
 // sources, give or take one, and neighbouring indices.  An entry is the
 // tile's place in the group (bits 15 and up) and the position's offset in
 // its tile.
-constexpr int kFlush = 1024;
+constexpr int kFlush = kThreads * 4;
 
 template <class F>
 __device__ __forceinline__ void scan_group(uint64_t t0, int ntile, const uint32_t *bits,
