@@ -778,17 +778,22 @@ __device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDe
 // sources, give or take one, and neighbouring indices.  An entry is the
 // tile's place in the group (bits 15 and up) and the position's offset in
 // its tile.
+//
+// The list's entry count alternates between two counters, gcnt[gp] and
+// gcnt[gp ^ 1] (gp: the block's current one, kept by the caller across
+// calls; both counters start at zero with the kernel): a flush zeroes the
+// other counter, whose last readers read it before the previous flush's
+// closing barrier, so a flushed round costs two barriers (the count's and
+// the flush's), not a reset with barriers of its own.
 constexpr int kFlush = kThreads * 4;
 
 template <class F>
 __device__ __forceinline__ void scan_group(uint64_t t0, int ntile, const uint32_t *bits,
-                                           uint64_t nbits, uint32_t *list, int *list_n, F &&f,
-                                           int lo = 0, int hi = kTileWords) {
+                                           uint64_t nbits, uint32_t *list, int *gcnt, int &gp,
+                                           F &&f, int lo = 0, int hi = kTileWords) {
   const uint64_t nwords = (nbits + 31) >> 5;
   const int lane = threadIdx.x & 31;
   const bool mine = threadIdx.x * 4 >= lo && threadIdx.x * 4 < hi;
-  if (threadIdx.x == 0) *list_n = 0;
-  __syncthreads();
   for (int g = 0; g < ntile; g++) {
     const uint64_t t = t0 + g;
     const uint64_t w0 = t * kTileWords + threadIdx.x * 4;
@@ -814,8 +819,9 @@ __device__ __forceinline__ void scan_group(uint64_t t0, int ntile, const uint32_
         const int y = __shfl_up_sync(0xffffffffu, incl, d);
         if (lane >= d) incl += y;
       }
+      int *cnt = gcnt + gp;
       int base = 0;
-      if (lane == 31 && incl) base = atomicAdd(list_n, incl);
+      if (lane == 31 && incl) base = atomicAdd(cnt, incl);
       base = __shfl_sync(0xffffffffu, base, 31);
       int pos = base + incl - c;
 #pragma unroll
@@ -827,18 +833,21 @@ __device__ __forceinline__ void scan_group(uint64_t t0, int ntile, const uint32_
         }
       }
       const int more = __syncthreads_or((w[0] | w[1] | w[2] | w[3]) != 0);
-      const int n = min(*list_n, kListCap);
-      // every thread has read the count before the next tile appends
-      __syncthreads();
+      const int n = min(*cnt, kListCap);
       if (more || n >= kFlush || g == ntile - 1) {
+        if (threadIdx.x == 0) gcnt[gp ^ 1] = 0;
         int e0, e1;
         my_share(n, e0, e1);
         for (int e = e0; e < e1; e++) {
           const uint32_t v = list[e];
           f((t0 + (v >> 15)) * (uint64_t)(kTileWords * 32) + (v & 32767u));
         }
+        // every entry is read (and the count by everyone) before the next
+        // round appends, on the other counter
         __syncthreads();
-        if (threadIdx.x == 0) *list_n = 0;
+        gp ^= 1;
+      } else {
+        // every thread has read the count before the next tile appends
         __syncthreads();
       }
       if (!more) break;
@@ -855,19 +864,29 @@ struct SparseSmem {
   uint32_t list2[kListCap];     // verify: survivors of the quick test
   int list_n;
   int n2[2];
+  int gcnt[2];                  // scatter: the list's two alternating counts
 };
+
+// The scatter's alternating counts start at zero (before the kernel's
+// first barrier); gp selects the current one.
+__device__ __forceinline__ void init_gcnt(SparseSmem &S) {
+  if (threadIdx.x == 0) {
+    S.gcnt[0] = 0;
+    S.gcnt[1] = 0;
+  }
+}
 
 // Tiles [t0, t0 + ntile) of predecessors_worker (tb8gen.c:484-516): every
 // source's unmoves marked (within each tile only the words [lo, hi)).
 template <int NS>
-__device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem &S, uint64_t t0,
-                                                  int ntile, DevStatus *st, int lo = 0,
-                                                  int hi = kTileWords) {
+__device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem &S, int &gp,
+                                                  uint64_t t0, int ntile, DevStatus *st,
+                                                  int lo = 0, int hi = kTileWords) {
   const DMat &M = c_mats[J.mat];
   bb set[NS];
   RowCache rc;
   scan_group(
-      t0, ntile, J.src, J.nbits, S.list, &S.list_n,
+      t0, ntile, J.src, J.nbits, S.list, S.gcnt, gp,
       [&](uint64_t idx) {
         const bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
         mark_unmoves_inc<NS>(J, S.kd, M, S.bin, set, occ, idx, st);
@@ -893,6 +912,8 @@ k_predecessors(SliceJob J, DevStatus *st, int nsplit, int gt) {
   __shared__ SparseSmem S;
   load_dests(J, S.kd);
   load_binomials(S.bin);
+  init_gcnt(S);
+  int gp = 0;
   __syncthreads();
   const uint64_t tiles = tiles_of(J.nbits);
   if (nsplit > 1) {
@@ -901,14 +922,14 @@ k_predecessors(SliceJob J, DevStatus *st, int nsplit, int gt) {
       uint64_t t;
       int lo, hi;
       part_of(u, nsplit, t, lo, hi);
-      tile_predecessors<NS>(J, S, t, 1, st, lo, hi);
+      tile_predecessors<NS>(J, S, gp, t, 1, st, lo, hi);
     }
     return;
   }
   const uint64_t nu = (tiles + gt - 1) / gt;
   for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
     const uint64_t t0 = u * gt;
-    tile_predecessors<NS>(J, S, t0, (int)min((uint64_t)gt, tiles - t0), st);
+    tile_predecessors<NS>(J, S, gp, t0, (int)min((uint64_t)gt, tiles - t0), st);
   }
 }
 
