@@ -70,12 +70,12 @@ __device__ __forceinline__ void tile_stream(const Op &o, uint64_t t) {
 }
 
 template <int NS>
-__device__ __forceinline__ void tile_sparse(const Op &o, SparseSmem &S, int &gp, uint64_t t,
-                                            DevStatus *st) {
+__device__ __forceinline__ void tile_sparse(const Op &o, SparseSmem &S, int &gp, uint32_t &ph,
+                                            uint64_t t, DevStatus *st) {
   switch (o.kind) {
   case OP_SCATTER: {
     const uint64_t t0 = t * o.gt, tiles = tiles_of(o.J.nbits);
-    tile_predecessors<NS>(o.J, S, gp, t0, (int)min((uint64_t)o.gt, tiles - t0), st);
+    tile_predecessors<NS>(o.J, S, gp, ph, t0, (int)min((uint64_t)o.gt, tiles - t0), st);
     break;
   }
   case OP_SCATTER_SUB: tile_predecessors_sub<NS>(o.J, S, t, st); break;
@@ -93,7 +93,9 @@ k_batch(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, uin
   __shared__ int s_op, s_abort;
   load_binomials(S.bin);
   init_gcnt(S);
+  bulk_init(S.B);
   int gp = 0;        // the scatter list's current count (scan_group)
+  uint32_t ph = 0;   // the staged tiles' barrier phases (scan_group)
   int cur_op = -1;   // the op whose descriptor (and king destinations) are in `so`
   int prev_op = -1;  // thread 0: the op of the item this block finished last
   for (;;) {
@@ -152,12 +154,12 @@ k_batch(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, uin
       tile_stream(so, t);
     } else {
       switch (so.ns) {
-      case 1: tile_sparse<1>(so, S, gp, t, st); break;
-      case 2: if (NSMAX >= 2) tile_sparse<(NSMAX >= 2 ? 2 : 1)>(so, S, gp, t, st); break;
-      case 3: if (NSMAX >= 3) tile_sparse<(NSMAX >= 3 ? 3 : 1)>(so, S, gp, t, st); break;
-      case 4: if (NSMAX >= 4) tile_sparse<(NSMAX >= 4 ? 4 : 1)>(so, S, gp, t, st); break;
-      case 5: if (NSMAX >= 5) tile_sparse<(NSMAX >= 5 ? 5 : 1)>(so, S, gp, t, st); break;
-      default: if (NSMAX >= 6) tile_sparse<(NSMAX >= 6 ? 6 : 1)>(so, S, gp, t, st); break;
+      case 1: tile_sparse<1>(so, S, gp, ph, t, st); break;
+      case 2: if (NSMAX >= 2) tile_sparse<(NSMAX >= 2 ? 2 : 1)>(so, S, gp, ph, t, st); break;
+      case 3: if (NSMAX >= 3) tile_sparse<(NSMAX >= 3 ? 3 : 1)>(so, S, gp, ph, t, st); break;
+      case 4: if (NSMAX >= 4) tile_sparse<(NSMAX >= 4 ? 4 : 1)>(so, S, gp, ph, t, st); break;
+      case 5: if (NSMAX >= 5) tile_sparse<(NSMAX >= 5 ? 5 : 1)>(so, S, gp, ph, t, st); break;
+      default: if (NSMAX >= 6) tile_sparse<(NSMAX >= 6 ? 6 : 1)>(so, S, gp, ph, t, st); break;
       }
     }
     // counted done at the top of the next iteration, after its barrier

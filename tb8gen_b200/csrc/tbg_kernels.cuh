@@ -771,6 +771,74 @@ __device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDe
   }
 }
 
+// ------------------------------------------------------ bulk tile staging
+// A scatter tile's words come into shared memory by the copy engine
+// (cp.async.bulk, completing on an mbarrier), the next tile of an item
+// while the block processes the current one.  The phase bits of the two
+// buffers' barriers (bit b: the parity buffer b's next copy completes) are
+// kept by the kernel in a register, the same in every thread.  The source is this GPU's own
+// memory and nothing is multicast.  Every wait is bounded: a copy that has
+// not landed after kBulkPolls polls is reported (status 5) and the block
+// reads its tiles with plain loads from then on.
+#ifndef TBG_BULK
+#define TBG_BULK 1
+#endif
+constexpr long kBulkPolls = 1L << 22;
+
+struct BulkStage {
+  uint4 buf[2][kThreads];       // two tiles of kTileWords words
+  unsigned long long bar[2];    // their mbarriers
+  int off;                      // a wait ran out: plain loads only
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void bulk_init(BulkStage &B) {
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 2; b++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&B.bar[b])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    B.off = 0;
+  }
+}
+
+// Thread 0: tile t of a bitmap of `words` 32-bit words (a multiple of 16:
+// bitmaps are 64-byte rounded) into buffer b.  The block's earlier reads of
+// that buffer are done (a barrier lies between them and this call).
+__device__ __forceinline__ void bulk_issue(BulkStage &B, int b, const uint32_t *bits,
+                                           uint64_t words, uint64_t t) {
+  const uint64_t w0 = t * kTileWords;
+  const uint32_t bytes = (uint32_t)(min((uint64_t)kTileWords, words - w0) * 4);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&B.bar[b])),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(&B.buf[b][0])),
+      "l"(bits + w0), "r"(bytes), "r"(smem_addr(&B.bar[b]))
+      : "memory");
+}
+
+// Every thread: waits (bounded) for buffer b's copy; false if it ran out.
+__device__ __forceinline__ bool bulk_wait(BulkStage &B, int b, uint32_t ph, DevStatus *st) {
+  const uint32_t parity = (ph >> b) & 1u;
+  for (long n = 0; n < kBulkPolls; n++) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_addr(&B.bar[b])), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  report(st, 5, (unsigned)b, 0);
+  return false;
+}
+
 // The sources of tiles [t0, t0 + ntile) of bits[] (within each tile only
 // its words [lo, hi)), gathered into one shared list until it holds
 // kFlush entries (or a tile's sources do not fit), then handed to f(idx)
@@ -790,15 +858,32 @@ constexpr int kFlush = kThreads * 4;
 template <class F>
 __device__ __forceinline__ void scan_group(uint64_t t0, int ntile, const uint32_t *bits,
                                            uint64_t nbits, uint32_t *list, int *gcnt, int &gp,
-                                           F &&f, int lo = 0, int hi = kTileWords) {
+                                           BulkStage &B, uint32_t &ph, DevStatus *st, F &&f,
+                                           int lo = 0, int hi = kTileWords) {
   const uint64_t nwords = (nbits + 31) >> 5;
+  const uint64_t words64 = ((nbits + 511) >> 9) << 4;  // the 64-byte rounded bitmap
   const int lane = threadIdx.x & 31;
   const bool mine = threadIdx.x * 4 >= lo && threadIdx.x * 4 < hi;
+  const bool bulk = TBG_BULK && !B.off;
+  if (bulk && threadIdx.x == 0) bulk_issue(B, 0, bits, words64, t0);
   for (int g = 0; g < ntile; g++) {
     const uint64_t t = t0 + g;
     const uint64_t w0 = t * kTileWords + threadIdx.x * 4;
+    const int b = g & 1;
+    // the next tile's copy, into the buffer every thread finished reading
+    // before the last tile's first barrier
+    if (bulk && g + 1 < ntile && threadIdx.x == 0) bulk_issue(B, b ^ 1, bits, words64, t + 1);
+    bool staged = false;
+    if (bulk) {
+      staged = bulk_wait(B, b, ph, st);
+      ph ^= 1u << b;
+      if (!staged && threadIdx.x == 0) B.off = 1;
+    }
     uint32_t w[4];
-    if (w0 + 4 <= nwords) {
+    if (staged) {
+      const uint4 v = w0 + 4 <= words64 ? B.buf[b][threadIdx.x] : make_uint4(0, 0, 0, 0);
+      w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+    } else if (w0 + 4 <= nwords) {
       const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(bits + w0));
       w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
     } else {
@@ -865,6 +950,7 @@ struct SparseSmem {
   int list_n;
   int n2[2];
   int gcnt[2];                  // scatter: the list's two alternating counts
+  __align__(128) BulkStage B;   // scatter: staged source tiles
 };
 
 // The scatter's alternating counts start at zero (before the kernel's
@@ -880,13 +966,14 @@ __device__ __forceinline__ void init_gcnt(SparseSmem &S) {
 // source's unmoves marked (within each tile only the words [lo, hi)).
 template <int NS>
 __device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem &S, int &gp,
-                                                  uint64_t t0, int ntile, DevStatus *st,
-                                                  int lo = 0, int hi = kTileWords) {
+                                                  uint32_t &ph, uint64_t t0, int ntile,
+                                                  DevStatus *st, int lo = 0,
+                                                  int hi = kTileWords) {
   const DMat &M = c_mats[J.mat];
   bb set[NS];
   RowCache rc;
   scan_group(
-      t0, ntile, J.src, J.nbits, S.list, S.gcnt, gp,
+      t0, ntile, J.src, J.nbits, S.list, S.gcnt, gp, S.B, ph, st,
       [&](uint64_t idx) {
         const bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
         mark_unmoves_inc<NS>(J, S.kd, M, S.bin, set, occ, idx, st);
@@ -913,7 +1000,9 @@ k_predecessors(SliceJob J, DevStatus *st, int nsplit, int gt) {
   load_dests(J, S.kd);
   load_binomials(S.bin);
   init_gcnt(S);
+  bulk_init(S.B);
   int gp = 0;
+  uint32_t ph = 0;
   __syncthreads();
   const uint64_t tiles = tiles_of(J.nbits);
   if (nsplit > 1) {
@@ -922,14 +1011,14 @@ k_predecessors(SliceJob J, DevStatus *st, int nsplit, int gt) {
       uint64_t t;
       int lo, hi;
       part_of(u, nsplit, t, lo, hi);
-      tile_predecessors<NS>(J, S, gp, t, 1, st, lo, hi);
+      tile_predecessors<NS>(J, S, gp, ph, t, 1, st, lo, hi);
     }
     return;
   }
   const uint64_t nu = (tiles + gt - 1) / gt;
   for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
     const uint64_t t0 = u * gt;
-    tile_predecessors<NS>(J, S, gp, t0, (int)min((uint64_t)gt, tiles - t0), st);
+    tile_predecessors<NS>(J, S, gp, ph, t0, (int)min((uint64_t)gt, tiles - t0), st);
   }
 }
 
