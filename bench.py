@@ -73,6 +73,11 @@ def parse():
     ap.add_argument("--path", default="batched", choices=["plain", "batched"])
     ap.add_argument("--ctas-per-sm", type=int, default=0,
                     help="persistent-kernel CTAs per SM (0: autotune)")
+    ap.add_argument("--profile-run", default="none", choices=["none", "plain", "batched"],
+                    help="ply workloads: one more step of that path, after all timing, "
+                         "between cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--mode", type=int, default=0, choices=[0, 1, 2],
+                    help="persistent kernel: 1 block-wide, 2 warp-wide work items (0: autotune)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="probe workload: target CPU time of the reference probe sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -275,17 +280,19 @@ def run_engine(a, rank, world, local):
                 e1.record(stream)
                 ev[ph].append((e0, e1))
 
-    # the same step recorded once; mode 0 = one launch per call, 1 = persistent
+    # the same step recorded once; mode 0 = one launch per call, 1 and 2 =
+    # persistent (block-wide or warp-wide work items, picked by the autotuner)
     from tb8gen_b200.plyjob import record_step
     nops, nitems = record_step(jobs)
-    mode = 1 if a.path == "batched" else 0
 
     def time_mode(md, reps):
         return time_batch(tbg, stream, md, reps)
 
     # autotune the persistent launch on this batch: CTAs per SM x tiles per
     # scatter work item
-    tune, best_cps, best_gt, nitems = autotune(tbg, time_mode, a.ctas_per_sm)
+    tune, best_mode, best_cps, best_gt, nitems = autotune(
+        tbg, time_mode, a.ctas_per_sm, (a.mode,) if a.mode else (1, 2))
+    mode = best_mode if a.path == "batched" else 0
 
     def step():
         tbg.batch_run(mode)
@@ -318,12 +325,20 @@ def run_engine(a, rank, world, local):
 
     # both paths on the same recorded batch, and per-phase device times
     plain_ms = time_mode(0, max(2, a.steps // 2))
-    batched_ms = time_mode(1, max(2, a.steps // 2))
+    batched_ms = time_mode(best_mode, max(2, a.steps // 2))
     for _ in range(max(3, a.steps // 2)):
         direct_step(timed_phases=True)
     torch.cuda.synchronize()
     phase_ms = {ph: statistics.median(e0.elapsed_time(e1) for e0, e1 in ev[ph])
                 for ph in phase_names}
+
+    if a.profile_run != "none":
+        # one extra step outside every timed region, bracketed for a profiler
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        tbg.batch_run(0 if a.profile_run == "plain" else best_mode)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
 
     counts = [j.counts() for j in jobs[:4]]
     mix = None
@@ -343,8 +358,9 @@ def run_engine(a, rank, world, local):
     per_pos = {"w_scatter": 0.125, "w_epilogue": 0.5, "l_scatter": 0.125, "l_verify": 0.25}
     kname = {"w_scatter": "k_predecessors", "w_epilogue": "k_epilogue_W",
              "l_scatter": "k_predecessors", "l_verify": "k_check_successors"}
-    if mode == 1:
-        dom, dom_ms, alg = "k_batch", ms, ALG_BYTES_PER_POS * positions
+    if mode != 0:
+        dom = "k_batch" if mode == 1 else "k_batch_w"
+        dom_ms, alg = ms, ALG_BYTES_PER_POS * positions
     else:
         ph = max(phase_ms, key=phase_ms.get)
         dom, dom_ms, alg = kname[ph], phase_ms[ph], per_pos[ph] * positions
@@ -387,7 +403,7 @@ def run_engine(a, rank, world, local):
         "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
         "paths_ms": {"plain": round(plain_ms, 4), "batched": round(batched_ms, 4),
                      "batched_speedup": round(plain_ms / batched_ms, 3)},
-        "batch": {"calls": nops, "work_items": nitems, "ctas_per_sm": best_cps,
+        "batch": {"calls": nops, "work_items": nitems, "mode": best_mode, "ctas_per_sm": best_cps,
                   "tiles_per_item": {"predecessors": best_gt[0], "candidates": best_gt[1]},
                   "autotune_ms": tune},
         "counts_first_jobs": counts,
@@ -408,7 +424,7 @@ def embedded(line):
 
 def time_batch(tbg, stream, md, reps):
     """Device time (ms) of one run of the selected recorded batch: mode 0
-    one launch per call, mode 1 the persistent launch."""
+    one launch per call, mode 1 or 2 the persistent launch."""
     import torch
 
     tbg.batch_run(md)
@@ -423,29 +439,37 @@ def time_batch(tbg, stream, md, reps):
     return e0.elapsed_time(e1) / reps
 
 
-TUNE_CPS = (3, 4, 6, 8)
-TUNE_SCATTER_TILES = (1, 2)
-TUNE_CANDIDATE_TILES = (1, 2, 4, 8)
+# the autotuner's grid per persistent mode: CTAs per SM, tiles per work
+# item of the W scatter, tiles per work item of the L candidates
+TUNE_GRID = {
+    1: ((4, 8), (1, 2), (1, 2, 4)),
+    2: ((4,), (1, 2), (1, 2, 4)),
+}
 
 
-def autotune(tbg, time_mode, fixed_cps=0):
+def autotune(tbg, time_mode, fixed_cps=0, modes=(1, 2)):
     """The persistent launch's shape picked on the recorded batch by its own
-    device time: CTAs per SM (the blocks that take work items at once) x
+    device time: the mode (1: block-wide work items, 2: one part of an item
+    per warp) x CTAs per SM (the blocks that take work items at once) x
     tiles per work item of the W step's scatter x tiles per work item of
-    the L step's candidates (the sources a block gathers before handing
-    them out).  Returns ({"<cps>x<w>x<l>": ms}, cps, (w, l), work items)."""
+    the L step's candidates (the sources a block, or a warp, gathers before
+    handing them out).  Returns ({"<mode>:<cps>x<w>x<l>": ms}, mode, cps,
+    (w, l), work items)."""
     tune = {}
-    for gw in TUNE_SCATTER_TILES:
-        for gl in TUNE_CANDIDATE_TILES:
-            tbg.batch_shape(gw, gl)
-            for cps in ((fixed_cps,) if fixed_cps > 0 else TUNE_CPS):
-                tbg.batch_tune(cps)
-                tune[f"{cps}x{gw}x{gl}"] = round(time_mode(1, 2), 4)
+    for md in modes:
+        cpss, gws, gls = TUNE_GRID[md]
+        for gw in gws:
+            for gl in gls:
+                tbg.batch_shape(gw, gl)
+                for cps in ((fixed_cps,) if fixed_cps > 0 else cpss):
+                    tbg.batch_tune(cps)
+                    tune[f"{md}:{cps}x{gw}x{gl}"] = round(time_mode(md, 2), 4)
     best = min(tune, key=tune.get)
-    cps, gw, gl = (int(x) for x in best.split("x"))
+    md, shape = best.split(":")
+    cps, gw, gl = (int(x) for x in shape.split("x"))
     nitems = tbg.batch_shape(gw, gl)
     tbg.batch_tune(cps)
-    return tune, cps, (gw, gl), nitems
+    return tune, int(md), cps, (gw, gl), nitems
 
 
 def mix_record(a, stream, slot=2):
@@ -471,10 +495,10 @@ def mix_record(a, stream, slot=2):
     try:
         nops, _ = record_step(jobs)
         tm = lambda md, reps: time_batch(tbg, stream, md, reps)
-        tune, cps, gt, nitems = autotune(tbg, tm)
+        tune, md, cps, gt, nitems = autotune(tbg, tm)
         reps = max(2, min(a.steps, 5))
         plain = tm(0, reps)
-        batched = tm(1, reps)
+        batched = tm(md, reps)
         tbg.sync()
     finally:
         tbg.batch_select(0)
@@ -496,7 +520,7 @@ def mix_record(a, stream, slot=2):
            "materials": sorted(pools), "plain_ms": round(plain, 3),
            "batched_ms": round(batched, 3), "batched_speedup": round(plain / batched, 3),
            "value_batched": round(positions / (batched / 1e3), 1),
-           "calls": nops, "work_items": nitems, "ctas_per_sm": cps,
+           "calls": nops, "work_items": nitems, "mode": md, "ctas_per_sm": cps,
            "tiles_per_item": {"predecessors": gt[0], "candidates": gt[1]},
            "autotune_ms": tune,
            "parity": {"golden": ("differ" if bad else "equal") if checked else "not recorded",

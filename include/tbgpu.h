@@ -266,7 +266,10 @@ int tbg_batch_end(int *nops, uint64_t *nitems);
  * per recorded call in record order (the plain path); mode 1 runs all of
  * them in one persistent kernel fed by a device work queue, each call
  * starting tile by tile as soon as the calls it depends on (by buffer) are
- * done.  Both give the same bitmaps as the calls made one by one. */
+ * done; mode 2 is the same persistent kernel with every work item cut into
+ * one part per warp, each warp taking parts on its own (no block barrier
+ * between a tile's sources).  All give the same bitmaps as the calls made
+ * one by one. */
 int tbg_batch_run(int mode);
 
 /* Epilogue counts of the last run, in record order (waits, bounded). */

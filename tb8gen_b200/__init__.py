@@ -287,7 +287,9 @@ def batch_end():
 
 
 def batch_run(mode: int):
-    """mode 0: one launch per recorded call; mode 1: one persistent launch."""
+    """mode 0: one launch per recorded call; mode 1: one persistent launch
+    (block-wide work items); mode 2: one persistent launch, each work item
+    cut into one part per warp."""
     check(lib().tbg_batch_run(mode))
 
 

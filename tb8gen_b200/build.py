@@ -15,7 +15,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libtbgpu.so")
-SOURCES = ["tbg_api.cu", "tbg_noalloc.cu", "tbg_probe_api.cu", "tbg_table.cpp", "tbg_subtable.cu"]
+SOURCES = ["tbg_api.cu", "tbg_persist_block.cu", "tbg_persist_warp.cu", "tbg_noalloc.cu",
+           "tbg_probe_api.cu", "tbg_table.cpp", "tbg_subtable.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
     "-shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-diag-suppress", "550",

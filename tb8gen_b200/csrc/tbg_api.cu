@@ -11,7 +11,8 @@
 
 #include "../../include/tbgpu.h"
 #include "tbg_host.h"
-#include "tbg_batch.cuh"
+#include "tbg_kernels.cuh"
+#include "tbg_persist.h"
 
 namespace tbg {
 
@@ -208,6 +209,8 @@ int Engine::add_material(const int *pt, int num) {
   for (int i = 0; i < num; i++) m.pt[i] = pt[i];
   m.num = num;
   cudaError_t e = cudaMemcpyToSymbol(c_mats, &d, sizeof d, nmats * sizeof(DMat));
+  if (e == cudaSuccess) e = persist_block_set_mat(d, nmats);
+  if (e == cudaSuccess) e = persist_warp_set_mat(d, nmats);
   if (e != cudaSuccess) return cuda_fail(e, "upload material");
   // a legacy-stream upload: complete before a non-blocking stream reads it
   CK(cudaStreamSynchronize(0));
@@ -238,6 +241,8 @@ int Engine::ensure_device() {
   int mod = 3;
   CK(cudaMemcpyToSymbol(c_stub_seed, &seed, sizeof seed));
   CK(cudaMemcpyToSymbol(c_stub_mod, &mod, sizeof mod));
+  CK(persist_block_set_stub(seed, mod, nullptr));
+  CK(persist_warp_set_stub(seed, mod, nullptr));
   // legacy-stream set-up, complete before any stream of the caller's
   // (blocking or not) launches
   CK(cudaDeviceSynchronize());
@@ -463,6 +468,8 @@ extern "C" int tbg_set_stub(uint64_t seed, int modulus) {
                              g_eng.stream));
   CK(cudaMemcpyToSymbolAsync(c_stub_mod, &modulus, sizeof modulus, 0, cudaMemcpyHostToDevice,
                              g_eng.stream));
+  CK(persist_block_set_stub(seed, modulus, g_eng.stream));
+  CK(persist_warp_set_stub(seed, modulus, g_eng.stream));
   CK(cudaStreamSynchronize(g_eng.stream));
   return TBG_OK;
 }
@@ -527,28 +534,14 @@ static uint32_t op_tiles(Op &o) {
 }
 
 static int launch_op(const Op &o) {
-  const int ns = o.ns;
   cudaStream_t st = g_eng.stream;
   switch (o.kind) {
-  case OP_SCATTER: {
-    const int sp = o.gt > 1 ? 1 : g_eng.split_for(o.ntiles, g_eng.bps_scatter);
-    NS_SWITCH(ns, k_predecessors<NS><<<g_eng.grid_for((uint64_t)o.ntiles * sp, g_eng.bps_scatter),
-                                       kThreads, 0, st>>>(o.J, g_eng.d_status, sp, o.gt));
-    return g_eng.check_launch("k_predecessors");
-  }
-  case OP_SCATTER_SUB: {
-    const int sp = g_eng.split_for(o.ntiles, g_eng.bps_scatter);
-    NS_SWITCH(ns, k_predecessors_sub<NS><<<g_eng.grid_for((uint64_t)o.ntiles * sp, g_eng.bps_scatter),
-                                           kThreads, 0, st>>>(o.J, g_eng.d_status, sp));
-    return g_eng.check_launch("k_predecessors_sub");
-  }
-  case OP_VERIFY: {
-    const int sp = g_eng.split_for(o.ntiles, g_eng.bps_verify);
-    NS_SWITCH(ns, k_check_successors<NS><<<g_eng.grid_for((uint64_t)o.ntiles * sp, g_eng.bps_verify),
-                                           kThreads, 0, st>>>(o.J, g_eng.d_status, o.out,
-                                                              o.out_words, sp));
-    return g_eng.check_launch("k_check_successors");
-  }
+  case OP_SCATTER:
+  case OP_SCATTER_SUB:
+  case OP_VERIFY:
+    // warp-wide sub-items of 32 words (k_op_w, tbg_persist_warp.cu)
+    persist_warp_launch_op(o, g_eng.num_sms * TBG_MINB_SCATTER, st, g_eng.d_status);
+    return g_eng.check_launch("k_op_w");
   case OP_EPILOGUE: {
     uint64_t n16 = o.n16;
     k_epilogue_W<<<g_eng.grid_for((n16 + kThreads - 1) / kThreads, 8), kThreads, 0, st>>>(
@@ -1114,16 +1107,18 @@ extern "C" int tbg_batch_run(int mode) {
     }
     return TBG_OK;
   }
-  if (mode != 1) return fail(TBG_ERR_ARG, "mode 0 (one launch per call) or 1 (persistent)");
+  if (mode != 1 && mode != 2)
+    return fail(TBG_ERR_ARG, "mode 0 (one launch per call), 1 or 2 (persistent)");
   CK(cudaMemsetAsync(b.d_done, 0, b.ops.size() * sizeof(unsigned int), st));
   CK(cudaMemsetAsync(b.d_next, 0, sizeof(unsigned long long), st));
   int grid = g_eng.num_sms * b.ctas_per_sm;
-  if (b.nsmax <= 3)
-    k_batch<3><<<grid, kThreads, 0, st>>>(b.d_ops, (int)b.ops.size(), b.d_preds, b.total, b.d_next,
-                                          b.d_done, g_eng.d_status, b.spin_limit);
-  else
-    k_batch<6><<<grid, kThreads, 0, st>>>(b.d_ops, (int)b.ops.size(), b.d_preds, b.total, b.d_next,
-                                          b.d_done, g_eng.d_status, b.spin_limit);
+  const PersistArgs pa{b.d_ops, (int)b.ops.size(), b.d_preds, b.total,
+                       b.d_next, b.d_done, g_eng.d_status, b.spin_limit};
+  if (mode == 2) {
+    persist_warp_launch(b.nsmax, grid, st, pa);
+    return g_eng.check_launch("k_batch_w");
+  }
+  persist_block_launch(b.nsmax, grid, st, pa);
   return g_eng.check_launch("k_batch");
 }
 

@@ -38,10 +38,12 @@ constexpr int kTileWords = kThreads * 4;      // 1024 words = 32768 positions at
 constexpr int kListCap = kThreads * 16;
 
 // Materials and stub parameters, uniform across a launch: constant memory.
-// (This header is compiled into exactly one translation unit, tbg_api.cu.)
-__constant__ DMat c_mats[TBG_MAX_MATS];
-__constant__ uint64_t c_stub_seed;
-__constant__ int c_stub_mod;
+// Every translation unit that includes this header (tbg_api.cu and the two
+// persistent-kernel units, tbg_persist_block.cu and tbg_persist_warp.cu)
+// holds its own copy; the host writes all of them (tbg_persist.h).
+static __constant__ DMat c_mats[TBG_MAX_MATS];
+static __constant__ uint64_t c_stub_seed;
+static __constant__ int c_stub_mod;
 
 // ------------------------------------------------------------------ ranks
 // Rank of a position given as kings + sets, with up to two per-set bit
@@ -75,6 +77,41 @@ __device__ __forceinline__ uint64_t rank_mod(const DIdx &X, const uint32_t *bin,
     }
   }
   return idx;
+}
+
+// Code that few positions reach is compiled out of line (TBG_COLD, on by
+// default), so that the hot loops of the persistent kernel -- whose warps
+// run different ops at once -- stay within the instruction cache.  The sets
+// travel by value (a struct), which keeps the caller's set[] in registers.
+#ifndef TBG_COLD
+#define TBG_COLD 1
+#endif
+#if TBG_COLD
+#define TBG_COLD_FN __noinline__
+#else
+#define TBG_COLD_FN __forceinline__
+#endif
+
+template <int NS>
+struct SetsV {
+  bb s[NS];
+};
+
+template <int NS>
+__device__ __forceinline__ SetsV<NS> sets_v(const bb *set) {
+  SetsV<NS> v;
+#pragma unroll
+  for (int k = 0; k < NS; k++) v.s[k] = set[k];
+  return v;
+}
+
+// rank_mod for the rare paths: king steps into a transformed slice, the
+// diagonal double mark, sets of more than four pieces.
+template <int NS>
+__device__ TBG_COLD_FN uint64_t rank_mod_cold(const DIdx &X, const uint32_t *bin, int k0, int k1,
+                                              SetsV<NS> v, int ka, bb xa, int kb, bb xb,
+                                              int mirror, int flip) {
+  return rank_mod<NS>(X, bin, k0, k1, v.s, ka, xa, kb, xb, mirror, flip);
 }
 
 // ------------------------------------------------------- incremental ranks
@@ -610,10 +647,21 @@ __device__ __forceinline__ int free_rank(int q, bb occ) {
 // (downward), Pascal's rule, i being q's place in its set; no other term
 // changes.  `kings`: the king squares before the move.
 template <int NS>
+__device__ __forceinline__ uint64_t seg_delta(const DIdx &X, const uint32_t *bin, const bb *set,
+                                              bb kings, int j0, bb betw, bool up);
+
+template <int NS>
 __device__ __forceinline__ uint64_t cross_delta(const DIdx &X, const uint32_t *bin,
                                                 const bb *set, bb kings, int j0, int a, int b) {
-  const bb betw = between(a, b);
-  const bool up = a < b;
+  return seg_delta<NS>(X, bin, set, kings, j0, between(a, b), a < b);
+}
+
+// The same sum over the squares of `betw` only (the move's squares lie on
+// one side: up, or down): a slider's index along a ray adds the terms of the
+// squares between one target and the next.
+template <int NS>
+__device__ __forceinline__ uint64_t seg_delta(const DIdx &X, const uint32_t *bin, const bb *set,
+                                              bb kings, int j0, bb betw, bool up) {
   bb occ = kings;
   uint64_t d = 0;
 #pragma unroll
@@ -710,11 +758,13 @@ __device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDe
     const uint64_t i =
         (D.mirror == 0 && D.flip == 0)
             ? idx + cross_delta<NS>(X, bin, set, kings, 0, me, D.to)
-            : rank_mod<NS>(X, bin, D.k0, D.k1, set, -1, 0, -1, 0, D.mirror, D.flip);
+            : rank_mod_cold<NS>(X, bin, D.k0, D.k1, sets_v<NS>(set), -1, 0, -1, 0, D.mirror,
+                                D.flip);
     mark(D.bits, i, X.size, st);
     if (D.dbl) {
       // mirror_diagonal (tb8gen.c:240-244) of the normalised position
-      const uint64_t i2 = rank_mod<NS>(X, bin, D.k0, D.k1, set, -1, 0, -1, 0, D.mirror, D.flip ^ 1);
+      const uint64_t i2 = rank_mod_cold<NS>(X, bin, D.k0, D.k1, sets_v<NS>(set), -1, 0, -1, 0,
+                                            D.mirror, D.flip ^ 1);
       mark(D.bits, i2, X.size, st);
     }
   }
@@ -733,9 +783,58 @@ __device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDe
         auto index_of = [&](int to) -> uint64_t {
           return inc ? base + (uint64_t)mover_rank(mv, bin, to, occk) * X.factor[k] +
                            cross_delta<NS>(X, bin, set, kings, k + 1, x, to)
-                     : rank_mod<NS>(X, bin, J.k0, J.k1, set, k, bit(x) | bit(to), -1, 0, 0, 0);
+                     : rank_mod_cold<NS>(X, bin, J.k0, J.k1, sets_v<NS>(set), k,
+                                         bit(x) | bit(to), -1, 0, 0, 0);
         };
-        if (J.filter != nullptr && type >= 3 && type <= 5) {
+        if (inc && type >= 3 && type <= 5) {
+          // A slider's targets along each ray, each index updated from the
+          // previous square's: the occupied squares below the target (for
+          // its rank among the free squares) and the other pieces of its set
+          // below it change by the squares passed in square order, and so
+          // does the later sets' term sum (seg_delta).  Same indices as
+          // mover_rank + cross_delta.
+          const bb others = set[k] & ~bit(x);
+          const int cnt0 = __popcll(occk & (bit(x) - 1)), pos0 = __popcll(others & (bit(x) - 1));
+          const int d0 = type == 3 ? 4 : 0, d1 = type == 4 ? 4 : 8;
+          for (int d = d0; d < d1; d++) {
+            // directions: 0 E, 1 W, 2 N, 3 S, 4 NE, 5 NW, 6 SE, 7 SW
+            const int df = (d == 0 || d == 4 || d == 6) ? 1 : (d == 1 || d == 5 || d == 7) ? -1 : 0;
+            const int dr = (d == 2 || d == 4 || d == 5) ? 1 : (d == 3 || d == 6 || d == 7) ? -1 : 0;
+            const bool up = dr > 0 || (dr == 0 && df > 0);
+            int f = x & 7, r = x >> 3, n = 0, cur = x, cnt = cnt0, pos = pos0;
+            uint64_t dx = 0, i_prev = 0, i_first = 0;
+            for (;;) {
+              f += df;
+              r += dr;
+              if ((unsigned)f > 7u || (unsigned)r > 7u) break;
+              const int to = r * 8 + f;
+              if ((occ >> to) & 1) break;
+              const bb seg = between(cur, to);
+              const int sc = __popcll(occk & seg), so = __popcll(others & seg);
+              cnt += up ? sc : -sc;
+              pos += up ? so : -so;
+              if (seg) dx += seg_delta<NS>(X, bin, set, kings, k + 1, seg, up);
+              cur = to;
+              uint32_t g = mv.g[0];
+#pragma unroll
+              for (int p = 1; p < 4; p++)
+                if (pos == p) g = mv.g[p];
+              const uint64_t i =
+                  base + (uint64_t)(bin[(pos + 1) * 64 + (to - cnt)] + g) * X.factor[k] + dx;
+              if (J.filter == nullptr) {
+                mark(J.self, i, X.size, st);
+              } else if (n == 0) {
+                i_first = i;
+              } else {
+                if (n == 1 && test(J.filter, i, X.size, st)) mark(J.self, i_first, X.size, st);
+                if (test(J.filter, i_prev, X.size, st)) mark(J.self, i, X.size, st);
+              }
+              i_prev = i;
+              n++;
+            }
+            if (J.filter != nullptr && n == 1) mark(J.self, i_first, X.size, st);
+          }
+        } else if (J.filter != nullptr && type >= 3 && type <= 5) {
           const int d0 = type == 3 ? 4 : 0, d1 = type == 4 ? 4 : 8;
           for (int d = d0; d < d1; d++) {
             // directions: 0 E, 1 W, 2 N, 3 S, 4 NE, 5 NW, 6 SE, 7 SW
@@ -1154,6 +1253,15 @@ __device__ __forceinline__ bool refute(const SliceJob &J, const KingDest *kd, co
   return false;
 }
 
+// refute for the candidates that pass the quick test (out of line, TBG_COLD).
+template <int NS>
+__device__ TBG_COLD_FN bool refute_cold(const SliceJob &J, const KingDest *kd, const DMat &M,
+                                        const uint32_t *bin, SetsV<NS> v, bb occ,
+                                        DevStatus *st) {
+  RowCache rc;
+  return refute<NS>(J, kd, M, bin, v.s, occ, rc, st);
+}
+
 // The quick test of the verify: the first quiet move of the side's pieces,
 // last set first, must lead into "wins".  Returns false when that refutes the
 // candidate, true when the candidate needs the full check.
@@ -1203,7 +1311,7 @@ __device__ __forceinline__ void tile_check(const SliceJob &J, SparseSmem &S, uin
       },
       [&](uint64_t idx) {
         bb occ = unrank_cached<NS>(M.ii, S.bin, idx, J.k0, J.k1, set, rc);
-        return refute<NS>(J, S.kd, M, S.bin, set, occ, rc, st);
+        return refute_cold<NS>(J, S.kd, M, S.bin, sets_v<NS>(set), occ, st);
       },
       out, lo, hi);
   if (out != nullptr && t == 0 && lo == 0) {
@@ -1432,6 +1540,9 @@ __device__ __forceinline__ uint32_t popc4(uint4 v) {
   return __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
 }
 
+// The plain (non-template) kernels below are defined in tbg_api.cu only; the
+// persistent-kernel units include this header for its device functions.
+#ifndef TBG_PERSIST_UNIT
 // Fused W-step epilogue (tb8gen.c:1072-1077): T &= ~wins; cnt += popcount(T)
 // below nbits; wins |= T.  One pass, 16-B loads and stores; 4 * N/8 bytes.
 // wins_in may equal wins_out (the reference's in-place form).
@@ -1544,5 +1655,7 @@ __global__ void __launch_bounds__(kThreads) k_gen_bernoulli(uint32_t *p, uint64_
     p[w] = v;
   }
 }
+
+#endif  // TBG_PERSIST_UNIT
 
 }  // namespace tbg

@@ -30,8 +30,9 @@
  * overlap the kernels of the segment between them.
  *
  * In resident mode each half-ply is recorded as one batch and run by the
- * persistent kernel (tbg_batch_run mode 1); -P launches every call on its
- * own instead, in the reference's call order.
+ * persistent kernel (tbg_batch_run mode 2, warp-wide work items; -k 1 for
+ * the block-wide mode 1); -P launches every call on its own instead, in the
+ * reference's call order.
  *
  * -o dir writes the reference's per-ply files under dir (n/W/<c>/<wk><bk>,
  * n/L/..., 0/L and, at the end, 0/wins; write_data's zstd frames), so that
@@ -187,6 +188,7 @@ static void illegal_and_mate(void)
  * kernel whose work queue follows the calls' buffer dependencies) unless -P
  * asks for one launch per call. */
 static int g_plain;
+static int g_kmode = 2;   /* persistent kernel: tbg_batch_run mode (-k) */
 
 static void batch_begin(void)
 {
@@ -199,7 +201,7 @@ static void batch_run(void)
   int nops;
   uint64_t items;
   ok(tbg_batch_end(&nops, &items), "batch end");
-  ok(tbg_batch_run(1), "batch run");
+  ok(tbg_batch_run(g_kmode), "batch run");
 }
 
 /* Ones in the slices of a plane: one strided count when the slices lie at
@@ -903,7 +905,7 @@ static void compute(const Part *P, int h, int64_t q)
     int nops;
     uint64_t items;
     ok(tbg_batch_end(&nops, &items), "batch end");
-    ok(tbg_batch_run(1), "batch run");
+    ok(tbg_batch_run(g_kmode), "batch run");
     if (nc) ok(tbg_batch_counts_async(hcnt + ncnt, nc), "counts");
     g_recording = 0;
   }
@@ -1114,7 +1116,7 @@ int main(int argc, char **argv)
   uint64_t seed = 1;
   int mod = 3, opt, force_stream = 0, max_ply = 1 << 30;
   double budget_mb = 0;
-  while ((opt = getopt(argc, argv, "s:m:qb:SHPpn:g:o:c:")) != -1) {
+  while ((opt = getopt(argc, argv, "s:m:qb:SHPpn:g:o:c:k:")) != -1) {
     if (opt == 's') seed = strtoull(optarg, NULL, 10);
     else if (opt == 'm') mod = atoi(optarg);
     else if (opt == 'q') quiet = 1;
@@ -1127,16 +1129,21 @@ int main(int argc, char **argv)
     else if (opt == 'g') g_seg = atoi(optarg);
     else if (opt == 'o') g_outdir = optarg;
     else if (opt == 'c') g_nsum = atoi(optarg);
+    else if (opt == 'k') g_kmode = atoi(optarg);
   }
   if (optind >= argc) {
     fprintf(stderr,
             "usage: tbgen [-s seed] [-m 3|5] [-b device_MB] [-S [-H]] [-g steps] [-P] [-p] [-n max_ply] "
-            "[-o dir] [-c slices] "
+            "[-o dir] [-c slices] [-k 1|2] "
             "MATERIAL\n");
     return EXIT_FAILURE;
   }
   if (g_seg < 0 || g_seg > MAX_SEG) {
     fprintf(stderr, "tbgen: -g takes 1..%d steps per segment (0: automatic)\n", MAX_SEG);
+    return EXIT_FAILURE;
+  }
+  if (g_kmode != 1 && g_kmode != 2) {
+    fprintf(stderr, "tbgen: -k takes 1 (block-wide) or 2 (warp-wide work items)\n");
     return EXIT_FAILURE;
   }
   if (g_nsum < 0 || g_nsum > NS) {

@@ -303,7 +303,7 @@ def output_digests(outputs: dict) -> dict:
 def record_step(jobs):
     """Records one step of every job (phase by phase: all W scatters, all
     epilogues, all L scatters, all verifies) as a batch; returns
-    (recorded calls, work items).  tbg.batch_run(0 | 1) then runs it."""
+    (recorded calls, work items).  tbg.batch_run(0 | 1 | 2) then runs it."""
     tbg.batch_begin()
     try:
         for ph in SlicePly.PHASES:

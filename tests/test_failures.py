@@ -107,12 +107,13 @@ def _job(tbg):
 
 
 @pytest.mark.gpu
-def test_dependency_wait_runs_out(gpu):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_dependency_wait_runs_out(gpu, mode):
     torch, tbg = gpu
     job = _job(tbg)
     try:
         tbg.batch_tune(4, DEFAULT_SPIN)
-        tbg.batch_run(1)
+        tbg.batch_run(mode)
         tbg.sync()
         want = {k: v.cpu().numpy().copy() for k, v in job.outputs().items()}
         failed = 0
@@ -120,7 +121,7 @@ def test_dependency_wait_runs_out(gpu):
             tbg.batch_tune(4, 1)
             job.T.fill_(0xA5)
             job.X.fill_(0x5A)
-            tbg.batch_run(1)
+            tbg.batch_run(mode)
             with pytest.raises(tbg.TbgError) as ei:
                 tbg.sync(20000)
             assert ei.value.code == TBG_ERR_DEVICE
@@ -129,7 +130,7 @@ def test_dependency_wait_runs_out(gpu):
         assert failed == 3
         # the status word is cleared, the next run with the normal limit is right
         tbg.batch_tune(4, DEFAULT_SPIN)
-        tbg.batch_run(1)
+        tbg.batch_run(mode)
         tbg.sync()
         got = {k: v.cpu().numpy() for k, v in job.outputs().items()}
         assert all(np.array_equal(got[k], want[k]) for k in want)

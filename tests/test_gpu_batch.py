@@ -1,6 +1,7 @@
 """The batched ply (tbg_batch_*): a recorded step of several slice-ply jobs
 of two materials gives the same bitmaps through one launch per call
-(mode 0) and through the persistent kernel (mode 1, several grid sizes),
+(mode 0) and through the persistent kernel (mode 1, block-wide work items,
+and mode 2, one part of an item per warp; several grid sizes),
 and each job's W, L and wins equal the reference's CPU workers on the same
 inputs."""
 import numpy as np
@@ -56,8 +57,8 @@ def run(torch, tbg, jobs, pools, mode, cps=2):
 def test_persistent_equals_plain(setup):
     torch, tbg, jobs, pools, nops = setup
     (a, sa), ca = run(torch, tbg, jobs, pools, 0)
-    for cps in (1, 2, 4):
-        (b, sb), cb = run(torch, tbg, jobs, pools, 1, cps)
+    for mode, cps in ((1, 1), (1, 2), (1, 4), (2, 1), (2, 2), (2, 4)):
+        (b, sb), cb = run(torch, tbg, jobs, pools, mode, cps)
         assert ca == cb
         for x, y in zip(a, b):
             for u, v in zip(x, y):
@@ -66,9 +67,10 @@ def test_persistent_equals_plain(setup):
             assert np.array_equal(sa[m][0], sb[m][0]) and np.array_equal(sa[m][1], sb[m][1])
 
 
-def test_batch_matches_reference(setup):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_batch_matches_reference(setup, mode):
     torch, tbg, jobs, pools, nops = setup
-    (b, _), counts = run(torch, tbg, jobs, pools, 1)
+    (b, _), counts = run(torch, tbg, jobs, pools, mode)
     for j, (T, X, W), c in zip(jobs, b, counts):
         O = orc.Ref(j.material, 8) if orc.ref_available() else orc.Port(j.material)
         O.set_stub(1)
@@ -184,7 +186,7 @@ def test_item_shapes_do_not_change_results(setup):
         for gw, gl in ((2, 4), (4, 8), (1, 16)):
             n = tbg.batch_shape(gw, gl)
             assert n > 0
-            for mode in (1, 0):
+            for mode in (1, 2, 0):
                 (b, sb), cb = run(torch, tbg, jobs, pools, mode, 3)
                 assert ca == cb
                 for x, y in zip(a, b):

@@ -64,9 +64,11 @@ def test_bench_slice_ply_equals_reference(env):
         tbg.sync()
         eng1 = {k: v.clone() for k, v in job.outputs().items()}
         counts1 = list(job.counts())
-        tbg.batch_run(0)
-        tbg.sync()
-        assert _diff(job.outputs(), {k: v.cpu().numpy() for k, v in eng1.items()}) == []
+        for mode in (0, 2):
+            tbg.batch_run(mode)
+            tbg.sync()
+            assert list(job.counts()) == counts1
+            assert _diff(job.outputs(), {k: v.cpu().numpy() for k, v in eng1.items()}) == []
         O = orc.Ref("KRRRvKRRR", CORES)
         O.set_stub(1, 3)
         cpu = CpuSlicePly(O, job, 1.0)
@@ -89,8 +91,8 @@ MIX_CASES = [("KQRvKRRR", 17, 0.001), ("KQRvKRRR", 452, 0.01), ("KQRvKRRR", 230,
              ("KQRRvKRR", 460, 0.05)]
 
 
-@pytest.mark.parametrize("shared", [False, True])
-def test_mix_materials_equal_reference(env, shared):
+@pytest.mark.parametrize("shared,mode", [(False, 1), (True, 1), (True, 2)])
+def test_mix_materials_equal_reference(env, shared, mode):
     """Slices of KQRvKRRR and KQRRvKRR at the mix densities, recorded in one
     batch and run by the persistent kernel, equal the reference's workers."""
     torch, tbg = env
@@ -105,7 +107,7 @@ def test_mix_materials_equal_reference(env, shared):
         jobs.append(SlicePly(mat, s, p, 2, pool))
     record_step(jobs)
     tbg.batch_tune(4)
-    tbg.batch_run(1)
+    tbg.batch_run(mode)
     tbg.sync()
     counts = tbg.batch_counts(len(jobs))
     for j, c in zip(jobs, counts):
