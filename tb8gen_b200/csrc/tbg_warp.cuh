@@ -34,6 +34,7 @@ static_assert(kSubWords == 128, "a sub-item is four words per lane");
 constexpr int kRing = 256;                      // a warp's source ring
 constexpr int kRing2 = 128;                     // verify: survivors of the quick test
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kRun = 4;                         // k_op_w: sub-items per run of a warp
 
 struct WarpSmem {
   Op op;                       // the op the warp runs: descriptor and king destinations
@@ -394,17 +395,24 @@ k_batch_w(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, u
   const int lane = threadIdx.x & 31;
   WarpSmem &S = W[threadIdx.x >> 5];
   const uint64_t total_w = total * kWarps;
+  int cur_op = -1;  // the op whose descriptor is in S.op
   unsigned long long it = warp_fetch(next);
   while (it < total_w) {
-    // the op of sub-item it, and its predecessors (lane 0 waits, bounded)
+    // the op of sub-item it (sub-items come in increasing order: the next
+    // op is found by stepping forward, or, far ahead, by a binary search),
+    // and its predecessors (lane 0 waits, bounded)
     const uint64_t b = it / kWarps;
-    int lo = 0, hi = nops - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (ops[mid].first <= b) lo = mid;
-      else hi = mid - 1;
+    int op = cur_op < 0 ? 0 : cur_op;
+    for (int n = 0; n < 4 && op + 1 < nops && ops[op + 1].first <= b; n++) op++;
+    if (op + 1 < nops && ops[op + 1].first <= b) {
+      int lo = op, hi = nops - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ops[mid].first <= b) lo = mid;
+        else hi = mid - 1;
+      }
+      op = lo;
     }
-    const int op = lo;
     int abort = 0;
     if (lane == 0) {
       const int np = ops[op].npred, po = ops[op].pred_off;
@@ -432,6 +440,7 @@ k_batch_w(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, u
       int4 *dst = reinterpret_cast<int4 *>(&S.op);
       for (int i = lane; i < (int)(sizeof(Op) / 16); i += 32) dst[i] = src[i];
     }
+    cur_op = op;
     __syncwarp();
     const uint64_t first_w = S.op.first * kWarps;
     const uint64_t end_w = first_w + (uint64_t)S.op.ntiles * kWarps;
@@ -467,10 +476,13 @@ k_batch_w(const Op *__restrict__ ops, int nops, const int *__restrict__ preds, u
 }
 
 // ---- one launch per call (the plain path and the per-call entry points)
-// One sparse op: its sub-items of 32 words cut into one contiguous run per
-// warp of the grid, each warp feeding its own ring, so that a lane batch
-// holds neighbouring positions (shared leading index digits, marks into one
-// target row).  The op is copied into shared memory once per block.
+// One sparse op: its sub-items of 32 words taken in runs of kRun
+// consecutive ones, the runs dealt to the grid's warps in turn, each warp
+// feeding its own ring.  Within a run a lane batch holds neighbouring
+// positions (shared leading index digits, marks into one target row);
+// across the grid the warps work on one window of the bitmap at a time
+// (warps x kRun x 1,024 positions), whose marks and reads stay in L2.
+// The op is copied into shared memory once per block.
 template <int NS, int KIND>
 __global__ void __launch_bounds__(kThreads, TBG_MINB_BATCH)
 k_op_w(const __grid_constant__ Op o, DevStatus *st, uint64_t nsub) {
@@ -486,21 +498,20 @@ k_op_w(const __grid_constant__ Op o, DevStatus *st, uint64_t nsub) {
   }
   __syncthreads();
   const int wid = threadIdx.x >> 5;
-  const uint64_t nw = (uint64_t)gridDim.x * kWarps;
-  const uint64_t run = (nsub + nw - 1) / nw;
-  const uint64_t g = (uint64_t)blockIdx.x * kWarps + wid;
-  const unsigned long long it = g * run;
+  const uint64_t skip = ((uint64_t)gridDim.x * kWarps - 1) * kRun;  // the other warps' runs
+  const unsigned long long it = ((uint64_t)blockIdx.x * kWarps + wid) * kRun;
   if (it >= nsub) return;
-  const uint64_t hi = it + run < nsub ? it + run : nsub;
-  auto fetch = [](unsigned long long cur) { return cur + 1; };
+  auto fetch = [skip](unsigned long long cur) {
+    return (cur + 1) % kRun ? cur + 1 : cur + 1 + skip;
+  };
   unsigned cnt = 0;
-  // sub-item numbers are op-relative (lo = 0); the run ends at hi
+  // sub-item numbers are op-relative (lo = 0)
   if (KIND == OP_SCATTER)
-    run_scatter<NS, 1>(so, bin, ring[wid], nullptr, it, 0, hi, fetch, st, cnt);
+    run_scatter<NS, 1>(so, bin, ring[wid], nullptr, it, 0, nsub, fetch, st, cnt);
   else if (KIND == OP_SCATTER_SUB)
-    run_scatter_sub<NS, 1>(so, bin, ring[wid], nullptr, it, 0, hi, fetch, st, cnt);
+    run_scatter_sub<NS, 1>(so, bin, ring[wid], nullptr, it, 0, nsub, fetch, st, cnt);
   else
-    run_verify<NS, 1>(so, bin, ring[wid], ring2[KIND == OP_VERIFY ? wid : 0], it, 0, hi, fetch,
+    run_verify<NS, 1>(so, bin, ring[wid], ring2[KIND == OP_VERIFY ? wid : 0], it, 0, nsub, fetch,
                       st, cnt);
 }
 

@@ -30,9 +30,10 @@
  * overlap the kernels of the segment between them.
  *
  * In resident mode each half-ply is recorded as one batch and run by the
- * persistent kernel (tbg_batch_run mode 2, warp-wide work items; -k 1 for
- * the block-wide mode 1); -P launches every call on its own instead, in the
- * reference's call order.
+ * persistent kernel (tbg_batch_run mode 1, block-wide work items: a
+ * half-ply's ~1,400 ops of small slices switch ops at every item, which a
+ * block pays once for its warps; -k 2 for warp-wide items); -P launches
+ * every call on its own instead, in the reference's call order.
  *
  * -o dir writes the reference's per-ply files under dir (n/W/<c>/<wk><bk>,
  * n/L/..., 0/L and, at the end, 0/wins; write_data's zstd frames), so that
@@ -188,7 +189,7 @@ static void illegal_and_mate(void)
  * kernel whose work queue follows the calls' buffer dependencies) unless -P
  * asks for one launch per call. */
 static int g_plain;
-static int g_kmode = 2;   /* persistent kernel: tbg_batch_run mode (-k) */
+static int g_kmode = 1;   /* persistent kernel: tbg_batch_run mode (-k) */
 
 static void batch_begin(void)
 {
