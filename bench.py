@@ -356,8 +356,8 @@ def run_engine(a, rank, world, local):
     # roofline of the dominant kernel: the persistent kernel on the batched
     # path (one launch per step), the slowest phase's kernel on the plain path
     per_pos = {"w_scatter": 0.125, "w_epilogue": 0.5, "l_scatter": 0.125, "l_verify": 0.25}
-    kname = {"w_scatter": "k_predecessors", "w_epilogue": "k_epilogue_W",
-             "l_scatter": "k_predecessors", "l_verify": "k_check_successors"}
+    kname = {"w_scatter": "k_op_w", "w_epilogue": "k_epilogue_W",
+             "l_scatter": "k_op_w", "l_verify": "k_op_w"}
     if mode != 0:
         dom = "k_batch" if mode == 1 else "k_batch_w"
         dom_ms, alg = ms, ALG_BYTES_PER_POS * positions

@@ -110,12 +110,6 @@ int tbg_set_stub(uint64_t seed, int modulus);
 int tbg_alloc(size_t bytes, void **dev);
 int tbg_free(void *dev);
 
-/* Launch tuning of the per-call sparse kernels (scatter, verify): a bitmap
- * of few 32768-position tiles is cut into up to max_split parts per tile
- * (a power of two, 1..64; default 64) so that every SM gets work.  Results
- * do not depend on it.  No counterpart in the reference. */
-int tbg_tune_split(int max_split);
-
 /* Copies between host memory and device memory on the library's stream,
  * returning when the copy is done: the host tier of a C host that keeps
  * slices in host memory (in place of kslice_read / kslice_write,

@@ -90,7 +90,6 @@ def lib():
             "tbg_probe_tune": [u64],
             "tbg_calc_sub_table": [i, i, vp * 5, C.POINTER(i), i, u64, i],
             "tbg_capture_material": [i, C.c_char_p, i],
-            "tbg_tune_split": [i],
             "tbg_probe_phase_ms": [i, C.POINTER(C.c_float), C.POINTER(u64)],
             "tbg_probe_stream_bytes": [i, i, C.POINTER(u64)],
             "tbg_probe_layout": [i, i, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)],
@@ -457,10 +456,6 @@ class DeviceTable:
 
     def decode(self, side: int, idx, squares):
         check(lib().tbg_decode_batch(self.handle, side, ptr(idx), idx.numel(), ptr(squares)))
-
-
-def tune_split(max_split: int):
-    check(lib().tbg_tune_split(max_split))
 
 
 def compact_queries(queries):

@@ -305,15 +305,6 @@ int Engine::grid_for(uint64_t units, int per_sm) {
   return g < 1 ? 1 : (int)g;
 }
 
-// Parts per tile for a bitmap of `tiles` tiles: the smallest power of two
-// (up to max_split) that gives every SM `per_sm` blocks.
-int Engine::split_for(uint64_t tiles, int per_sm) {
-  const uint64_t want = (uint64_t)num_sms * per_sm;
-  int sp = 1;
-  while (sp < max_split && tiles * sp < want) sp <<= 1;
-  return sp;
-}
-
 int Engine::check_launch(const char *what) {
   launches++;
   cudaError_t e = cudaGetLastError();
@@ -1162,13 +1153,6 @@ extern "C" int tbg_alloc(size_t bytes, void **dev) {
 extern "C" int tbg_free(void *dev) {
   if (!dev) return TBG_OK;
   CK(cudaFree(dev));
-  return TBG_OK;
-}
-
-extern "C" int tbg_tune_split(int max_split) {
-  if (max_split < 1 || max_split > 64 || (max_split & (max_split - 1)))
-    return fail(TBG_ERR_ARG, "max_split must be a power of two from 1 to 64");
-  g_eng.max_split = max_split;
   return TBG_OK;
 }
 

@@ -95,9 +95,6 @@ struct Engine {
   int nmats = 0;
   int cur = -1;
   uint64_t launches = 0;  // kernels launched by this library
-  int bps_scatter = 8;    // grid = SMs x this for the sparse kernels (tiles loop)
-  int bps_verify = 8;
-  int max_split = 64;     // parts per tile for small bitmaps (tbg_tune_split)
   int scatter_tiles = 0;    // tiles per predecessors work item (tbg_batch_shape; 0: 1)
   int candidate_tiles = 0;  // tiles per candidates work item (0: 4)
   // Recorded batches: kBatchSlots slots, one selected (tbg_batch_select).
@@ -123,7 +120,6 @@ struct Engine {
   int add_material(const int *pt, int num);
   int fill_job(SliceJob &J, int stm, int s, bool need_sub);
   int grid_for(uint64_t units, int per_sm);
-  int split_for(uint64_t tiles, int per_sm);
   int check_launch(const char *what);
   int wait(int timeout_ms);
   int tickets_ready();

@@ -1,19 +1,22 @@
-// The ply-step kernels (sm_100a).  All arithmetic is integer and bitwise.
+// The ply-step device code (sm_100a).  All arithmetic is integer and bitwise.
 //
-//  k_predecessors        predecessors_worker      tb8gen.c:484-527   (W step / L candidates)
-//  k_predecessors_sub    predecessors_sub_worker  tb8gen.c:346-414   (uncaptures)
-//  k_check_successors    check_successors_worker  tb8gen.c:607-661   (L-step verify)
+//  mark_unmoves_inc, mark_king_unmoves, mark_piece_unmoves
+//                        predecessors_worker      tb8gen.c:484-527   (W step / L candidates)
+//                        predecessors_sub_worker  tb8gen.c:346-414   (uncaptures)
+//  survives_quick, refute
+//                        check_successors_worker  tb8gen.c:607-661   (L-step verify)
 //  k_calc_sub            calc_sub_worker          tb8gen.c:280-342   (capture classes, seeded stub)
 //  k_calc_illegal        calc_illegal_worker      tb8gen.c:664-684
 //  k_calc_mate           calc_mate_worker         tb8gen.c:686-727
 //  k_epilogue_W          kslice_and_not + kslice_count + kslice_or  (tb8gen.c:1072-1077)
 //
-// Sparse kernels (the first three) walk the source bitmap in tiles of
-// TILE_WORDS 32-bit words: each thread loads 16 B (coalesced), the block
-// compacts the set bits of the tile into a shared-memory list, and the
-// threads then take list entries round-robin.  The list is drained in rounds,
-// so any density is handled; at the densities of a ply (1-5 %) one round
-// holds the whole tile and every thread gets one or two positions.
+// The per-position work of the sparse steps (the first three lines) is
+// driven by two schemes: warp-wide (tbg_warp.cuh: the per-call kernel k_op_w
+// and the persistent k_batch_w) and block-wide (the tile_* functions below,
+// run by the persistent k_batch of tbg_batch.cuh): each thread loads 16 B of
+// a tile of kTileWords 32-bit words (coalesced), the block compacts the set
+// bits of the tile into a shared-memory list, and the threads then take list
+// entries; the list is drained in rounds, so any density is handled.
 #pragma once
 
 #include "tbg_device.cuh"
@@ -771,15 +774,16 @@ __device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDe
   bb occk = kings;
 #pragma unroll
   for (int k = 0; k < NS; k++) {
+    const bb setk = set[k];
     if (M.set_color[k] == J.stm) {
       const bool inc = X.mult[k] <= 4;
-      const uint64_t base = idx - (uint64_t)rank_one(set[k], occk, bin) * X.factor[k];
+      const uint64_t base = idx - (uint64_t)rank_one(setk, occk, bin) * X.factor[k];
       const int type = M.set_type[k];
-      bb pcs = set[k];
+      bb pcs = setk;
       while (pcs) {
         const int x = pop_lsb(pcs);
         Mover mv;
-        if (inc) mover_init(mv, bin, set[k], x, occk);
+        if (inc) mover_init(mv, bin, setk, x, occk);
         auto index_of = [&](int to) -> uint64_t {
           return inc ? base + (uint64_t)mover_rank(mv, bin, to, occk) * X.factor[k] +
                            cross_delta<NS>(X, bin, set, kings, k + 1, x, to)
@@ -793,7 +797,7 @@ __device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDe
           // below it change by the squares passed in square order, and so
           // does the later sets' term sum (seg_delta).  Same indices as
           // mover_rank + cross_delta.
-          const bb others = set[k] & ~bit(x);
+          const bb others = setk & ~bit(x);
           const int cnt0 = __popcll(occk & (bit(x) - 1)), pos0 = __popcll(others & (bit(x) - 1));
           const int d0 = type == 3 ? 4 : 0, d1 = type == 4 ? 4 : 8;
           for (int d = d0; d < d1; d++) {
@@ -866,7 +870,7 @@ __device__ __forceinline__ void mark_unmoves_inc(const SliceJob &J, const KingDe
         }
       }
     }
-    occk |= set[k];
+    occk |= setk;
   }
 }
 
@@ -1080,47 +1084,6 @@ __device__ __forceinline__ void tile_predecessors(const SliceJob &J, SparseSmem 
       lo, hi);
 }
 
-// A tile of a small bitmap is cut into `nsplit` parts of consecutive words
-// (nsplit a power of two up to 64), one block each, so that a bitmap of few
-// tiles still occupies every SM; each part keeps its own words' results.
-__device__ __forceinline__ void part_of(uint64_t u, int nsplit, uint64_t &t, int &lo, int &hi) {
-  t = u / (uint64_t)nsplit;
-  const int r = (int)(u % (uint64_t)nsplit);
-  lo = r * (kTileWords / nsplit);
-  hi = lo + kTileWords / nsplit;
-}
-
-// Work units: with nsplit > 1 (a bitmap of few tiles) a part of a tile;
-// otherwise a group of gt consecutive tiles.
-template <int NS>
-__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER)
-k_predecessors(SliceJob J, DevStatus *st, int nsplit, int gt) {
-  __shared__ SparseSmem S;
-  load_dests(J, S.kd);
-  load_binomials(S.bin);
-  init_gcnt(S);
-  bulk_init(S.B);
-  int gp = 0;
-  uint32_t ph = 0;
-  __syncthreads();
-  const uint64_t tiles = tiles_of(J.nbits);
-  if (nsplit > 1) {
-    const uint64_t nu = tiles * (uint64_t)nsplit;
-    for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
-      uint64_t t;
-      int lo, hi;
-      part_of(u, nsplit, t, lo, hi);
-      tile_predecessors<NS>(J, S, gp, ph, t, 1, st, lo, hi);
-    }
-    return;
-  }
-  const uint64_t nu = (tiles + gt - 1) / gt;
-  for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
-    const uint64_t t0 = u * gt;
-    tile_predecessors<NS>(J, S, gp, ph, t0, (int)min((uint64_t)gt, tiles - t0), st);
-  }
-}
-
 // predecessors_sub_worker (tb8gen.c:346-394): the source is the sub bitmap
 // of captured set J.set (colour stm^1); each position is uncaptured by the
 // king and by every non-king piece of stm.
@@ -1145,22 +1108,6 @@ __device__ __forceinline__ void tile_predecessors_sub(const SliceJob &J, SparseS
                            return false;
                          },
                          nullptr, NoHook(), NoHook(), lo, hi);
-}
-
-template <int NS>
-__global__ void __launch_bounds__(kThreads, TBG_MINB_SCATTER) k_predecessors_sub(SliceJob J, DevStatus *st,
-                                                                                int nsplit) {
-  __shared__ SparseSmem S;
-  load_dests(J, S.kd);
-  load_binomials(S.bin);
-  __syncthreads();
-  const uint64_t nu = tiles_of(J.nbits) * (uint64_t)nsplit;
-  for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
-    uint64_t t;
-    int lo, hi;
-    part_of(u, nsplit, t, lo, hi);
-    tile_predecessors_sub<NS>(J, S, t, st, lo, hi);
-  }
 }
 
 // ----------------------------------------------------------- L step
@@ -1317,23 +1264,6 @@ __device__ __forceinline__ void tile_check(const SliceJob &J, SparseSmem &S, uin
   if (out != nullptr && t == 0 && lo == 0) {
     for (uint64_t w = ((J.nbits + 31) >> 5) + threadIdx.x; w < out_words; w += blockDim.x)
       out[w] = J.cand[w];
-  }
-}
-
-template <int NS>
-__global__ void __launch_bounds__(kThreads, TBG_MINB_VERIFY) k_check_successors(SliceJob J, DevStatus *st,
-                                                                  uint32_t *out,
-                                                                  uint64_t out_words, int nsplit) {
-  __shared__ SparseSmem S;
-  load_dests(J, S.kd);
-  load_binomials(S.bin);
-  __syncthreads();
-  const uint64_t nu = tiles_of(J.nbits) * (uint64_t)nsplit;
-  for (uint64_t u = blockIdx.x; u < nu; u += gridDim.x) {
-    uint64_t t;
-    int lo, hi;
-    part_of(u, nsplit, t, lo, hi);
-    tile_check<NS>(J, S, t, st, out, out_words, lo, hi);
   }
 }
 
