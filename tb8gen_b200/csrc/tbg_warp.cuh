@@ -163,6 +163,13 @@ __device__ __forceinline__ void store_cleared(uint32_t *dst, bool always, uint64
   }
 }
 
+// The sparse runners are compiled out of line (TBG_RUNNER): each gets its own
+// register allocation, as a kernel of one op kind would, instead of sharing
+// one across every kind the persistent kernel dispatches to.
+#ifndef TBG_RUNNER
+#define TBG_RUNNER __noinline__
+#endif
+
 // The sparse runners below process sub-items it, fetch(it), ... of one op
 // (those below hi: sub-items are handed out in increasing order) and return
 // the first sub-item at or past hi.  o: the op (in shared memory); ring,
@@ -170,7 +177,7 @@ __device__ __forceinline__ void store_cleared(uint32_t *dst, bool always, uint64
 
 // ---- scatter (predecessors_worker, tb8gen.c:484-516) and candidates
 template <int NS, int WPL, class Fetch>
-__device__ __forceinline__ unsigned long long run_scatter(const Op &o, const uint32_t *bin,
+__device__ TBG_RUNNER unsigned long long run_scatter(const Op &o, const uint32_t *bin,
                                                           uint64_t *ring, uint64_t *,
                                                           unsigned long long it, uint64_t lo,
                                                           uint64_t hi, Fetch &&fetch,
@@ -203,7 +210,7 @@ __device__ __forceinline__ unsigned long long run_scatter(const Op &o, const uin
 
 // ---- uncaptures (predecessors_sub_worker, tb8gen.c:346-394)
 template <int NS, int WPL, class Fetch>
-__device__ __forceinline__ unsigned long long run_scatter_sub(const Op &o, const uint32_t *bin,
+__device__ TBG_RUNNER unsigned long long run_scatter_sub(const Op &o, const uint32_t *bin,
                                                               uint64_t *ring, uint64_t *,
                                                               unsigned long long it, uint64_t lo,
                                                               uint64_t hi, Fetch &&fetch,
@@ -244,7 +251,7 @@ __device__ __forceinline__ unsigned long long run_scatter_sub(const Op &o, const
 // bit kept), and a candidate that survives both tests is set again; only
 // this warp touches the chunk's words.
 template <int NS, int WPL, class Fetch>
-__device__ __forceinline__ unsigned long long run_verify(const Op &o, const uint32_t *bin,
+__device__ TBG_RUNNER unsigned long long run_verify(const Op &o, const uint32_t *bin,
                                                          uint64_t *ring, uint64_t *ring2,
                                                          unsigned long long it, uint64_t lo,
                                                          uint64_t hi, Fetch &&fetch,
