@@ -50,7 +50,8 @@ def _tbgen():
 
 def test_tbgen_arguments_without_gpu():
     """The C host driver refuses bad arguments before it touches CUDA: no
-    material, and a segment size outside 0..64."""
+    material, a segment size outside 0..64, a persistent-kernel mode other
+    than 1 or 2."""
     import subprocess
 
     tbgen = _tbgen()
@@ -60,6 +61,9 @@ def test_tbgen_arguments_without_gpu():
         r = subprocess.run([tbgen, "-S", "-g", g, "KRvK"], capture_output=True, text=True,
                            timeout=60)
         assert r.returncode != 0 and "-g takes" in r.stderr
+    for k in ("0", "3"):
+        r = subprocess.run([tbgen, "-k", k, "KRvK"], capture_output=True, text=True, timeout=60)
+        assert r.returncode != 0 and "-k takes" in r.stderr
 
 
 def test_tbgen_reports_library_errors_without_gpu():
