@@ -7,9 +7,9 @@ tests/golden/make_schedule_golden.py).  KRvK and KQvK are the reference's
 real results (captures into KvK are draws); the others replace the 7-piece
 probe by the seeded stub on both sides.  KRvKN uses the five-valued stub, so
 cursed wins and blessed losses reach the ply-101 paths.  The resident
-driver runs each half-ply as one recorded batch (the persistent kernel);
-with -P it launches every call on its own: both must print the golden
-counts."""
+driver runs each half-ply as one recorded batch (the persistent kernel,
+block-wide work items; -k 2: warp-wide); with -P it launches every call on
+its own: all must print the golden counts."""
 import json
 import os
 import subprocess
@@ -26,14 +26,14 @@ with open(GOLDEN) as f:
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("path", ["batched", "plain"])
+@pytest.mark.parametrize("path", ["batched", "batched-warp", "plain"])
 @pytest.mark.parametrize("material", sorted(CASES))
 def test_generation_counts_match_reference(material, path):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     case = CASES[material]
-    cmd = [TBGEN] + (["-P"] if path == "plain" else [])
+    cmd = [TBGEN] + {"batched": [], "batched-warp": ["-k", "2"], "plain": ["-P"]}[path]
     if case["seed"] is not None:
         cmd += ["-s", str(case["seed"]), "-m", str(case["mod"])]
     r = subprocess.run(cmd + [material], capture_output=True, text=True, timeout=600)
